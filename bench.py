@@ -1,0 +1,514 @@
+#!/usr/bin/env python
+"""AO any-hit ray-query throughput on B200.
+
+Default workload (the batched configuration): 64 procedural scenes
+(heightfield + boxes family) with triangle counts log-uniform in [10k, 2M] and
+AO ray counts log-uniform in [256K, 8M] (cosine-weighted from uniform surface
+samples, tmin = 1e-4 diag, tmax = 0.1 diag), all traced any-hit in one
+persistent batch launch (Morton sort + CUDA graph, parameters from the
+autotuner), beside 64 plain per-scene launches of the same kernel family and
+the reference's own CWBVH kernel rebuilt for sm_100a.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rq|reference]
+                    [--workload batched|small] [--quick]
+
+One JSON line on rank 0.  Under torchrun each rank traces its own copy of
+the workload (weak scaling, no data-path collective); time is the max over
+ranks.  Rays and hits exceed L2 (inputs larger than L2 between steps).
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "AO any-hit Mrays/s on 1 B200, batched/served vs plain launch; p50/p99 latency"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------- workload --
+
+def workload_spec(name: str, quick: bool, rank: int):
+    rng = np.random.default_rng(12345)
+    if name == "small":
+        return [dict(seed=0, tris=10592, rays=1 << 20, small=True)]
+    n = 64 if not quick else 8
+    tris = np.exp(rng.uniform(math.log(10_000), math.log(2_000_000), 64)).astype(np.int64)[:n]
+    rays = np.exp(rng.uniform(math.log(256 * 1024), math.log(8 * 1024 * 1024), 64)).astype(np.int64)[:n]
+    if quick:
+        tris = np.minimum(tris, 200_000)
+        rays = np.minimum(rays, 1 << 20)
+    return [dict(seed=i + 100 * rank, tris=int(t), rays=int(r), small=False) for i, (t, r) in enumerate(zip(tris, rays))]
+
+
+def build_scenes(spec, threads_per_build: int = 1):
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+
+    def one(s):
+        V, I = W.heightfield_boxes(s["seed"]) if s["small"] else W.scene_of_size(s["seed"], s["tris"])
+        hb = rq.HostBVH(V, I, rq.CWBVH, threads=threads_per_build)
+        return V, I, hb
+
+    workers = max(1, min(len(spec), (os.cpu_count() or 1)))
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(one, spec))
+
+
+# ------------------------------------------------------------------ timing --
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                smax.append(float(f[2].split()[0]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def time_steps(fn, steps: int, warmup: int, stream, dist=None, flush=None) -> float:
+    """ms per step: CUDA events on `stream`, synchronize + barrier on both sides, max over ranks."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms
+
+
+def measured_peak_hbm():
+    try:
+        p = json.loads(PEAKS.read_text())
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(workload: str):
+    """DRAM bytes per launch of the trace kernel from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / f"traffic_{workload}.json"
+    try:
+        return json.loads(f.read_text())
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- CPU legs --
+
+def cpu_sample(spec, built, target_rays: int, seed: int = 7):
+    """A bounded sample of the workload on the host: rays from every scene,
+    proportionally to its ray count, generated with the host's numpy RNG."""
+    rng = np.random.default_rng(seed)
+    total = sum(s["rays"] for s in spec)
+    out = []
+    for s, (V, I, hb) in zip(spec, built):
+        k = max(64, int(round(target_rays * s["rays"] / total)))
+        tri = rng.integers(0, I.shape[0], k)
+        a = np.sqrt(rng.random(k)).astype(np.float32)
+        b = rng.random(k).astype(np.float32)
+        p0, p1, p2 = V[I[tri, 0]], V[I[tri, 1]], V[I[tri, 2]]
+        P = p0 * (1 - a)[:, None] + p1 * (b * a)[:, None] + p2 * (1 - (1 - a) - b * a)[:, None]
+        nrm = np.cross(p1 - p0, p2 - p0)
+        nrm /= np.maximum(np.linalg.norm(nrm, axis=1, keepdims=True), 1e-30)
+        u1, u2 = rng.random(k), rng.random(k)
+        r, ph = np.sqrt(u1), 2 * np.pi * u2
+        t1 = np.cross(nrm, [0.0, 0.0, 1.0])
+        short = np.linalg.norm(t1, axis=1) < 0.1
+        t1[short] = np.cross(nrm[short], [0.0, 1.0, 0.0])
+        t1 /= np.linalg.norm(t1, axis=1, keepdims=True)
+        t2 = np.cross(t1, nrm)
+        d = t1 * (r * np.cos(ph))[:, None] + t2 * (r * np.sin(ph))[:, None] + nrm * np.sqrt(1 - u1)[:, None]
+        dg = float(np.linalg.norm(V.max(0) - V.min(0)))
+        rays = np.zeros((k, 8), np.float32)
+        rays[:, 0:3], rays[:, 3] = P, 1e-4 * dg
+        rays[:, 4:7], rays[:, 7] = d, 0.1 * dg
+        out.append((hb, rays))
+    return out
+
+
+def time_cpu(sample, threads: int = 0) -> tuple[float, int]:
+    from oracle import pyoracle as po
+    n = sum(r.shape[0] for _, r in sample)
+    t0 = time.perf_counter()
+    for hb, rays in sample:
+        po.trace(0, hb.nodes, hb.woop, rays, True, threads=threads)
+    return time.perf_counter() - t0, n
+
+
+# ------------------------------------------------------------------ main --
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="rq", choices=["rq", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "small"])
+    ap.add_argument("--quick", action="store_true", help="8 smaller scenes (smoke runs)")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, world, rank, warmup)
+
+    import torch
+    import torch.distributed as tdist
+    import datetime
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local_rank))
+        dist = tdist
+
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+
+    spec = workload_spec(args.workload, args.quick, rank)
+    t0 = time.time()
+    built = build_scenes(spec)
+    log(f"[bench] built {len(spec)} scenes, {sum(s['tris'] for s in spec)/1e6:.1f}M tris in {time.time()-t0:.1f}s")
+
+    stream = torch.cuda.Stream()
+    ctx = rq.Context()
+    scenes, rays, hits = [], [], []
+    with torch.cuda.stream(stream):
+        for s, (V, I, hb) in zip(spec, built):
+            sc = rq.Scene.from_host(hb)
+            ds = W.DeviceScene(rq.CWBVH, hb, sc, torch.from_numpy(V).cuda(), torch.from_numpy(I).cuda(),
+                               W.diag(V), I.shape[0])
+            r = W.ao_rays(ds, s["rays"], seed=s["seed"] + 1000, stream=stream)
+            scenes.append(ds)
+            rays.append(r)
+            hits.append(torch.empty((s["rays"], 4), device="cuda"))
+    torch.cuda.synchronize()
+    total_rays = sum(s["rays"] for s in spec)
+    items = [(ds.scene, r, h) for ds, r, h in zip(scenes, rays, hits)]
+    log(f"[bench] {total_rays/1e6:.1f}M rays on device")
+
+    # ---- plain per-scene launches (the denominator of the batching target)
+    def plain():
+        for ds, r, h in zip(scenes, rays, hits):
+            rq.trace(ctx, ds.scene, r, h, rq.ANY, stream=stream)
+
+    ms_plain = time_steps(plain, args.steps, warmup, stream, dist)
+    ctx.check(stream)
+    plain_occ = [h[:, 1].view(torch.int32).ne(-1).sum().item() for h in hits]
+
+    # ---- batched: autotuned sort threshold / block size / stack depth, CUDA graph
+    cache = str(ROOT / "profiles" / "autotune_cache.txt") if os.environ.get("RQ_TUNE_CACHE") else None
+    t0 = time.time()
+    bp = rq.autotune_batch(ctx, items, rq.ANY, cache_path=cache, stream=stream)
+    log(f"[bench] autotune {time.time()-t0:.1f}s -> block {bp.launch.block_size} smem {bp.launch.smem_stack} "
+        f"sort_threshold {bp.sort_threshold} graph {bp.use_graph}")
+    batch = rq.Batch(ctx, items, rq.ANY, params=bp)
+    ms_batch = time_steps(lambda: batch.run(stream), args.steps, warmup, stream, dist)
+    ctx.check(stream)
+    batch_occ = [h[:, 1].view(torch.int32).ne(-1).sum().item() for h in hits]
+    occlusion_identical = plain_occ == batch_occ
+
+    # trace kernel alone (the dominant kernel) for the roofline
+    batch.run(stream)
+    ms_kernel = time_steps(lambda: rq.lib.rq_batch_run_stage(batch._h, 2, stream.cuda_stream), args.steps, warmup,
+                           stream, dist)
+    ms_sort = time_steps(lambda: rq.lib.rq_batch_run_stage(batch._h, 1, stream.cuda_stream), 3, 1, stream, dist)
+    launches_per_step = int(rq.lib.rq_batch_kernel_count(batch._h))
+
+    # ---- clocks during a timed batched region
+    clk = Clocks(torch.cuda.current_device())
+    ms_batch2 = time_steps(lambda: batch.run(stream), args.steps, 1, stream, dist)
+    clocks = clk.stop()
+
+    # ---- end to end through the public API with host buffers
+    host_rays = [torch.empty(r.shape, dtype=r.dtype, pin_memory=True) for r in rays]
+    host_hits = [torch.empty(h.shape, dtype=h.dtype, pin_memory=True) for h in hits]
+    for hr, r in zip(host_rays, rays):
+        hr.copy_(r)
+
+    def e2e():
+        for hr, r in zip(host_rays, rays):
+            r.copy_(hr, non_blocking=True)
+        batch.run(stream)
+        for hh, h in zip(host_hits, hits):
+            hh.copy_(h, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        ms_e2e = time_steps(e2e, args.steps, warmup, stream, dist)
+
+    # ---- algorithmic bytes per ray: 32 (ray) + 16 (hit) + 80 per node + 48 per triangle
+    nodes_total, tris_total = 0, 0
+    for ds, r in zip(scenes, rays):
+        hh = torch.empty((r.shape[0], 4), device="cuda")
+        nv, nt = rq.trace_counted(ctx, ds.scene, r, hh, rq.ANY, stream=stream)
+        nodes_total += int(nv.sum().item())
+        tris_total += int(nt.sum().item())
+        del hh, nv, nt
+    ctx.check(stream)
+    alg_bytes = 48 * total_rays + 80 * nodes_total + 48 * tris_total
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
+    traffic = profile_traffic(args.workload)
+
+    # ---- the reference's CWBVH kernel rebuilt for sm_100a, same rays (closest-hit: its only mode)
+    ref_gpu = None
+    if not args.no_ref_gpu:
+        ref_gpu = run_ref_gpu(scenes, rays, warmup=1, steps=2)
+
+    # ---- CPU baseline (oracle restatement, all host threads, bounded sample)
+    cpu = None
+    if rank == 0 and world >= 1:
+        cpu = cpu_baseline(spec, built)
+
+    world_rays = total_rays * world
+    value = world_rays / (ms_batch * 1e-3) / 1e6
+    line = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "Mrays/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": warmup,
+        "ms_per_step": round(ms_batch, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded procedural scenes and AO rays; the reference's mesh.dat/samplecache.dat are not shipped)",
+        "config": {
+            "workload": ("batched: 64 heightfield+box scenes, tris log-U[10k,2M], AO any-hit rays log-U[256K,8M], "
+                         "one persistent launch, Morton sort, CUDA graph, autotuned")
+            if args.workload == "batched" and not args.quick else f"{args.workload}{' (quick)' if args.quick else ''}",
+            "scenes": len(spec),
+            "triangles": int(sum(s["tris"] for s in spec)),
+            "rays_per_gpu": int(total_rays),
+            "query": "any-hit",
+            "layout": "CWBVH 80 B nodes, Woop 48 B triangles, Ray 32 B, Hit 16 B",
+            "launch": {"block": bp.launch.block_size, "smem_stack": bp.launch.smem_stack,
+                       "sort_threshold": int(bp.sort_threshold), "cuda_graph": bool(bp.use_graph)},
+            "l2": "inputs larger than L2 (rays+hits %.1f GB per step)" % (total_rays * 48 / 1e9),
+            "parallelism": f"replicas x{world} (rays independent, no data-path collective)",
+        },
+        "plain_per_scene": {"value": round(world_rays / (ms_plain * 1e-3) / 1e6, 2), "unit": "Mrays/s",
+                            "ms_per_step": round(ms_plain, 4), "launches_per_step": 2 * len(spec)},
+        "batched_vs_plain": round(ms_plain / ms_batch, 3),
+        "occlusion_identical_batched_vs_plain": occlusion_identical,
+        "stages_ms": {"sort": round(ms_sort, 4), "trace_kernel": round(ms_kernel, 4)},
+        "e2e": {"value": round(world_rays / (ms_e2e * 1e-3) / 1e6, 2), "unit": "Mrays/s",
+                "h2d_bytes_per_step": int(total_rays * 32), "d2h_bytes_per_step": int(total_rays * 16),
+                "ms_per_step": round(ms_e2e, 4)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": f"hbm_gbs of {peak_kind}",
+                     "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                     "algorithmic_bytes_per_launch": int(alg_bytes),
+                     "bytes_per_ray": round(alg_bytes / total_rays, 1),
+                     "nodes_per_ray": round(nodes_total / total_rays, 3),
+                     "tris_per_ray": round(tris_total / total_rays, 3)},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "clocks": clocks,
+        "clocks_ms_per_step": round(ms_batch2, 4),
+    }
+    if ref_gpu is not None:
+        line["reference_cwbvh_kernel_sm100a"] = ref_gpu
+        if ref_gpu.get("value"):
+            line["batched_vs_reference_kernel"] = round(value / world / ref_gpu["value"], 3)
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_ref_gpu(scenes, rays, warmup: int, steps: int):
+    """The reference's rtTraceCWBVH (oracle/_ref, compiled from its sources for
+    sm_100a, shipped 32x32x(32x2) grid) on the same scenes and rays."""
+    import torch
+    try:
+        from oracle import pyoracle as po
+        if not po.ref_available():
+            return {"unavailable": "oracle/_ref/libref.so not built"}
+        lib = po.ref()
+    except Exception as e:  # pragma: no cover
+        return {"unavailable": str(e)}
+    # The reference kernel has a 40-entry stack without an overflow check; a
+    # tree of depth d needs at most 2d entries.
+    deepest = max(ds.host.info["depth"] for ds in scenes)
+    if 2 * deepest > 40:
+        return {"unavailable": f"tree depth {deepest} could overflow the reference's 40-entry stack"}
+    import re
+    import tempfile
+    out_hits = [torch.empty((r.shape[0], 4), device="cuda") for r in rays]
+    total = sum(r.shape[0] for r in rays)
+    sys.stdout.flush()
+    tmp = tempfile.TemporaryFile(mode="w+b")
+    saved = os.dup(1)
+    try:
+        os.dup2(tmp.fileno(), 1)  # rtTraceCWBVH logs its own event-timed duration per call
+
+        def step():
+            for ds, r, h in zip(scenes, rays, out_hits):
+                dn, dw, dp = C_buffers(ds.scene)
+                lib.ref_bind_cwbvh(dn, dw, dp)
+                lib.ref_trace_cwbvh(r.data_ptr(), h.data_ptr(), r.shape[0])
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        torch.cuda.synchronize()
+        wall_ms = (time.perf_counter() - t0) * 1e3 / steps
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+    tmp.seek(0)
+    txt = tmp.read().decode(errors="replace")
+    tmp.close()
+    per_call = [float(m) for m in re.findall(r"([0-9.]+)MS, [0-9.]+MRays/s \(rtTraceCWBVH", txt)]
+    timed = per_call[len(per_call) - steps * len(rays):] if len(per_call) >= steps * len(rays) else []
+    ms = sum(timed) / steps if timed else wall_ms
+    return {"value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+            "wall_ms_per_step": round(wall_ms, 3),
+            "query": "closest-hit (the reference has no any-hit kernel)",
+            "timing": "sum of the reference's own CUDA-event kernel times (its log line per rtTraceCWBVH call)"
+            if timed else "host wall clock around synchronous rtTraceCWBVH calls",
+            "grid": "32x32 blocks of 32x2 threads (as shipped)"}
+
+
+def C_buffers(scene):
+    import ctypes as C
+    import cwbvh_b200 as rq
+    n, w, p = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    rq.check(rq.lib.rq_scene_device_buffers(scene._h, C.byref(n), C.byref(w), C.byref(p)), "rq_scene_device_buffers")
+    return n, w, p
+
+
+def cpu_baseline(spec, built):
+    try:
+        from oracle import pyoracle as po
+        threads = po.oracle().oracle_max_threads()
+    except Exception as e:
+        return {"unavailable": str(e)}
+    sample = cpu_sample(spec, built, target_rays=1 << 21)
+    time_cpu(sample[:2], threads)  # warm
+    dt, n = time_cpu(sample, threads)
+    if dt < 10.0:  # aim for >= 10 s of CPU work
+        reps = int(math.ceil(10.0 / max(dt, 1e-3)))
+        dt = 0.0
+        for _ in range(reps):
+            d, _ = time_cpu(sample, threads)
+            dt += d
+        n *= reps
+    return {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+            "sample": f"{n} AO any-hit rays drawn from all scenes in proportion to their ray counts, CWBVH, "
+                      f"oracle/oracle.c with OpenMP over {threads} threads, {dt:.1f}s"}
+
+
+def run_reference(args, world, rank, warmup):
+    """Reference arm: the reference has no CPU traversal, so its path is timed
+    through the C restatement (oracle/oracle.c, kind "port") on the host cores,
+    each step a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    spec = workload_spec(args.workload, args.quick, 0)
+    built = build_scenes(spec)
+    from oracle import pyoracle as po
+    threads = po.oracle().oracle_max_threads()
+    sample = cpu_sample(spec, built, target_rays=1 << 20)
+    for _ in range(min(warmup, 1)):
+        time_cpu(sample, threads)
+    dt, n = 0.0, 0
+    for _ in range(args.steps):
+        d, k = time_cpu(sample, threads)
+        dt += d
+        n += k
+    value = n / dt / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batched (bounded sample per step)" if args.workload == "batched" else args.workload},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
+                         "sample": f"{n // args.steps} rays per step from all scenes; the reference has no CPU "
+                                   f"traversal, its CWBVH algorithm restated in C (oracle/oracle.c)"},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,448 @@
+"""cwbvh_b200 -- a B200 ray-query engine for compressed wide BVHs.
+
+Python front end over librq.so (C ABI in include/rq.h).  Host BVH build and
+conversion run in C++; tracing, ray generation, sorting, batching and serving
+run in hand-written sm_100a CUDA kernels.  Device buffers are torch CUDA
+tensors (torch is used for device memory and streams only).
+
+Reference entry points mirrored here (names and argument meaning):
+  rtBindCWBVHData / rtTraceCWBVH   src/TraversalKernelCWBVH.h:3-11
+  rtBindBVH2Data  / rtTraceBVH2    src/TraversalKernelBVH2.h:3-11
+  GenerateAORaysUniform            src/ValidationKernels.h:3-9
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from ._native import ANY, BVH2, CLOSEST, CWBVH, Launch, RQError, check, lib
+
+__all__ = [
+    "ANY", "BVH2", "CLOSEST", "CWBVH", "Launch", "RQError", "HostBVH", "Scene", "Context", "Batch", "Server",
+    "trace", "trace_ordered", "trace_counted", "aorays", "sample_surfels", "ao_reduce", "sort_rays",
+    "autotune", "autotune_batch", "default_launch", "woopify", "gen_heightfield_boxes", "gen_city",
+    "gen_spheres_terrain", "rtBindCWBVHData", "rtTraceCWBVH", "rtBindBVH2Data", "rtTraceBVH2",
+    "rtOccludedCWBVH", "rtOccludedBVH2", "GenerateAORaysUniform", "version", "lib",
+]
+
+
+def version() -> str:
+    return lib.rq_version().decode()
+
+
+# ------------------------------------------------------------ helpers ----
+
+def _ptr(t) -> int:
+    """Device pointer of a torch CUDA tensor (must be contiguous)."""
+    if t is None:
+        return 0
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _rows(t, width: int, what: str) -> int:
+    n = t.numel() * t.element_size()
+    if n % (width * 4):
+        raise ValueError(f"{what}: byte size {n} is not a multiple of {width * 4}")
+    return n // (width * 4)
+
+
+# ------------------------------------------------------------- meshes ----
+
+def _take_mesh(v, nv, i, nt):
+    verts = np.ctypeslib.as_array(C.cast(v, C.POINTER(C.c_float)), shape=(nv.value * 3,)).copy().reshape(-1, 3)
+    idx = np.ctypeslib.as_array(C.cast(i, C.POINTER(C.c_int32)), shape=(nt.value * 3,)).copy().reshape(-1, 3)
+    lib.rq_free_mesh(v, i)
+    return verts, idx
+
+
+def gen_heightfield_boxes(seed: int = 0, grid: int = 64, n_boxes: int = 200, box_min: float = 0.01,
+                          box_max: float = 0.1):
+    """(grid+1)^2-vertex heightfield over [0,1]^2 (heights U[0,1]) plus boxes."""
+    v, i, nv, nt = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64()
+    check(lib.rq_gen_heightfield_boxes(seed, grid, n_boxes, box_min, box_max, C.byref(v), C.byref(nv), C.byref(i),
+                                       C.byref(nt)), "rq_gen_heightfield_boxes")
+    return _take_mesh(v, nv, i, nt)
+
+
+def gen_city(seed: int = 0, n_buildings: int = 10000):
+    v, i, nv, nt = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64()
+    check(lib.rq_gen_city(seed, n_buildings, C.byref(v), C.byref(nv), C.byref(i), C.byref(nt)), "rq_gen_city")
+    return _take_mesh(v, nv, i, nt)
+
+
+def gen_spheres_terrain(seed: int = 0, target_tris: int = 1_000_000):
+    v, i, nv, nt = C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64()
+    check(lib.rq_gen_spheres_terrain(seed, target_tris, C.byref(v), C.byref(nv), C.byref(i), C.byref(nt)),
+          "rq_gen_spheres_terrain")
+    return _take_mesh(v, nv, i, nt)
+
+
+def woopify(v0, v1, v2) -> np.ndarray:
+    """3 float4 Woop rows (V0, V1, V2) of one triangle, shape (3, 4)."""
+    a = [np.ascontiguousarray(x, dtype=np.float32) for x in (v0, v1, v2)]
+    out = np.zeros(12, np.float32)
+    check(lib.rq_woopify(*(x.ctypes.data for x in a), out.ctypes.data), "rq_woopify")
+    return out.reshape(3, 4)
+
+
+# ---------------------------------------------------------- host BVHs ----
+
+class HostBVH:
+    """A converted BVH in host memory (node / Woop / primitive-index buffers)."""
+
+    def __init__(self, vertices, indices, kind: int = CWBVH, max_leaf_size: int = 0, sah_bins: int = 0,
+                 max_depth: int = 0, threads: int = 0):
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        i = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1, 3)
+        self.vertices, self.indices, self.kind = v, i, kind
+        bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads)
+        h = C.c_void_p()
+        check(lib.rq_build_bvh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0], kind, C.byref(bp),
+                               C.byref(h)), "rq_build_bvh")
+        self._h = h
+        info = N.BVHInfo()
+        check(lib.rq_host_bvh_info(h, C.byref(info)), "rq_host_bvh_info")
+        self.info = {f: getattr(info, f) for f, _ in N.BVHInfo._fields_}
+        self.info["bounds_lo"] = tuple(info.bounds_lo)
+        self.info["bounds_hi"] = tuple(info.bounds_hi)
+        n, w, p = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib.rq_host_bvh_buffers(h, C.byref(n), C.byref(w), C.byref(p)), "rq_host_bvh_buffers")
+        self.nodes = np.ctypeslib.as_array(C.cast(n, C.POINTER(C.c_float)),
+                                           shape=(info.node_float4s * 4,)).copy().reshape(-1, 4)
+        self.woop = (np.ctypeslib.as_array(C.cast(w, C.POINTER(C.c_float)), shape=(info.woop_float4s * 4,))
+                     .copy().reshape(-1, 4) if info.woop_float4s else np.zeros((0, 4), np.float32))
+        self.prim_index = (np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int32)), shape=(info.prim_index_count,))
+                           .copy() if info.prim_index_count else np.zeros(0, np.int32))
+
+    def tree(self) -> dict:
+        """The pre-conversion tree (see rq_host_bvh_tree)."""
+        w, nn, nl, npr, rl = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        check(lib.rq_host_bvh_tree(self._h, C.byref(w), C.byref(nn), C.byref(nl), C.byref(npr), C.byref(rl),
+                                   None, None, None, None, None), "rq_host_bvh_tree")
+        W = w.value
+        codes = np.zeros((nn.value, W), np.int32)
+        boxes = np.zeros((nn.value, W, 6), np.float32)
+        lf = np.zeros(nl.value, np.int32)
+        lc = np.zeros(nl.value, np.int32)
+        refs = np.zeros(npr.value, np.int32)
+        check(lib.rq_host_bvh_tree(self._h, None, None, None, None, None, codes.ctypes.data, boxes.ctypes.data,
+                                   lf.ctypes.data, lc.ctypes.data, refs.ctypes.data), "rq_host_bvh_tree")
+        return {"width": W, "codes": codes, "boxes": boxes, "leaf_first": lf, "leaf_count": lc, "prim_refs": refs,
+                "root_is_leaf": bool(rl.value)}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_host_bvh_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+# ------------------------------------------------------- device state ----
+
+class Scene:
+    """A device-resident scene (node + Woop buffers in HBM)."""
+
+    def __init__(self, handle: C.c_void_p, kind: int, keep=None):
+        self._h = handle
+        self.kind = kind
+        self._keep = keep
+
+    @classmethod
+    def from_host(cls, hb: HostBVH) -> "Scene":
+        h = C.c_void_p()
+        check(lib.rq_scene_from_host_bvh(hb._h, C.byref(h)), "rq_scene_from_host_bvh")
+        return cls(h, hb.kind)
+
+    @classmethod
+    def from_arrays(cls, kind: int, nodes: np.ndarray, woop: np.ndarray, prim_index: Optional[np.ndarray] = None):
+        nodes = np.ascontiguousarray(nodes, np.float32)
+        woop = np.ascontiguousarray(woop, np.float32)
+        pi = None if prim_index is None else np.ascontiguousarray(prim_index, np.int32)
+        h = C.c_void_p()
+        check(lib.rq_scene_create(kind, nodes.ctypes.data, nodes.size // 4, woop.ctypes.data, woop.size // 4,
+                                  None if pi is None else pi.ctypes.data, 0 if pi is None else pi.size, 1,
+                                  C.byref(h)), "rq_scene_create")
+        return cls(h, kind)
+
+    @classmethod
+    def from_device(cls, kind: int, nodes, woop, prim_index=None) -> "Scene":
+        """Borrow device tensors (kept alive by the Scene object)."""
+        h = C.c_void_p()
+        check(lib.rq_scene_create(kind, _ptr(nodes), _rows(nodes, 4, "nodes"), _ptr(woop), _rows(woop, 4, "woop"),
+                                  _ptr(prim_index) or None, 0 if prim_index is None else prim_index.numel(), 0,
+                                  C.byref(h)), "rq_scene_create")
+        return cls(h, kind, keep=(nodes, woop, prim_index))
+
+    @property
+    def nbytes(self) -> int:
+        return int(lib.rq_scene_bytes(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Context:
+    """Device scratch for the persistent kernels (ray counter, error word)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib.rq_ctx_create(C.byref(h)), "rq_ctx_create")
+        self._h = h
+
+    def check(self, stream=None) -> None:
+        check(lib.rq_ctx_check(self._h, _stream(stream)), "rq_ctx_check")
+
+    def status(self, stream=None) -> int:
+        return int(lib.rq_ctx_check(self._h, _stream(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def default_launch(kind: int = CWBVH, query: int = ANY) -> Launch:
+    l = Launch()
+    check(lib.rq_default_launch(kind, query, C.byref(l)), "rq_default_launch")
+    return l
+
+
+# ------------------------------------------------------------ tracing ----
+
+def trace(ctx: Context, scene: Scene, rays, hits, query: int = ANY, launch: Optional[Launch] = None,
+          stream=None, count: Optional[int] = None) -> None:
+    """Trace rays (CUDA tensor, 32 B per ray) into hits (16 B per ray)."""
+    n = _rows(rays, 8, "rays") if count is None else count
+    check(lib.rq_trace(ctx._h, scene._h, _ptr(rays), _ptr(hits), n, query,
+                       C.byref(launch) if launch is not None else None, _stream(stream)), "rq_trace")
+
+
+def trace_ordered(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stream=None) -> None:
+    """Trace in the oracle's traversal order (bit-identical results)."""
+    check(lib.rq_trace_ordered(ctx._h, scene._h, _ptr(rays), _ptr(hits), _rows(rays, 8, "rays"), query,
+                               _stream(stream)), "rq_trace_ordered")
+
+
+def trace_counted(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stream=None):
+    """Trace and return per-ray (node fetches, triangle tests) as int32 tensors."""
+    import torch
+    n = _rows(rays, 8, "rays")
+    nv = torch.zeros(n, dtype=torch.int32, device=rays.device)
+    nt = torch.zeros(n, dtype=torch.int32, device=rays.device)
+    check(lib.rq_trace_counted(ctx._h, scene._h, _ptr(rays), _ptr(hits), n, query, _ptr(nv), _ptr(nt),
+                               _stream(stream)), "rq_trace_counted")
+    return nv, nt
+
+
+def aorays(pos, nrm, radius, spp: int, seed: int = 0, tmin: float = 0.01, tmax: float = 1e20,
+           offset_scale: float = 0.5, out=None, stream=None):
+    """AO rays from a surfel cache (pos/nrm float4 tensors, radius float or None)."""
+    import torch
+    ns = _rows(pos, 4, "pos")
+    if out is None:
+        out = torch.empty((ns * spp, 8), dtype=torch.float32, device=pos.device)
+    check(lib.rq_aorays(_ptr(pos), _ptr(nrm), _ptr(radius) or None, ns, spp, seed, tmin, tmax, offset_scale,
+                        _ptr(out), _stream(stream)), "rq_aorays")
+    return out
+
+
+def sample_surfels(vertices, indices, n: int, seed: int = 0, stream=None):
+    """n surfels at uniform (triangle, barycentric) points of a device mesh."""
+    import torch
+    dev = vertices.device
+    pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    rad = torch.empty((n,), dtype=torch.float32, device=dev)
+    nt = indices.numel() // 3
+    check(lib.rq_sample_surfels(_ptr(vertices), _ptr(indices), nt, n, seed, _ptr(pos), _ptr(nrm), _ptr(rad),
+                                _stream(stream)), "rq_sample_surfels")
+    return pos, nrm, rad
+
+
+def ao_reduce(hits, n_surfels: int, spp: int, stream=None):
+    import torch
+    ao = torch.empty(n_surfels, dtype=torch.float32, device=hits.device)
+    check(lib.rq_ao_reduce(_ptr(hits), n_surfels, spp, _ptr(ao), _stream(stream)), "rq_ao_reduce")
+    return ao
+
+
+def sort_rays(ctx: Context, rays, bounds_lo, bounds_hi, stream=None):
+    import torch
+    n = _rows(rays, 8, "rays")
+    out = torch.empty_like(rays)
+    perm = torch.empty(n, dtype=torch.int32, device=rays.device)
+    lo = (C.c_float * 3)(*bounds_lo)
+    hi = (C.c_float * 3)(*bounds_hi)
+    check(lib.rq_sort_rays(ctx._h, _ptr(rays), n, lo, hi, _ptr(out), _ptr(perm), _stream(stream)), "rq_sort_rays")
+    return out, perm
+
+
+def _items(items: Sequence[tuple]):
+    arr = (N.BatchItem * len(items))()
+    for k, (scene, rays, hits) in enumerate(items):
+        arr[k] = N.BatchItem(scene._h, _ptr(rays), _ptr(hits), _rows(rays, 8, "rays"))
+    return arr
+
+
+class Batch:
+    """Many (scene, rays, hits) items traced in one persistent launch."""
+
+    def __init__(self, ctx: Context, items: Sequence[tuple], query: int = ANY, launch: Optional[Launch] = None,
+                 sort_threshold: int = -1, use_graph: bool = False, params: Optional[N.BatchParams] = None):
+        self._keep = list(items)
+        arr = _items(items)
+        if params is None:
+            params = N.BatchParams(launch if launch is not None else Launch(), sort_threshold, int(use_graph))
+        self.params = params
+        h = C.c_void_p()
+        check(lib.rq_batch_create(ctx._h, arr, len(items), query, C.byref(params), C.byref(h)), "rq_batch_create")
+        self._h = h
+
+    def run(self, stream=None) -> None:
+        check(lib.rq_batch_run(self._h, _stream(stream)), "rq_batch_run")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def autotune(ctx: Context, scene: Scene, rays, hits, query: int = ANY, cache_path: Optional[str] = None,
+             stream=None) -> Launch:
+    l = Launch()
+    check(lib.rq_autotune(ctx._h, scene._h, _ptr(rays), _ptr(hits), _rows(rays, 8, "rays"), query,
+                          cache_path.encode() if cache_path else None, C.byref(l), _stream(stream)), "rq_autotune")
+    return l
+
+
+def autotune_batch(ctx: Context, items: Sequence[tuple], query: int = ANY, cache_path: Optional[str] = None,
+                   stream=None) -> N.BatchParams:
+    arr = _items(items)
+    bp = N.BatchParams()
+    check(lib.rq_autotune_batch(ctx._h, arr, len(items), query, cache_path.encode() if cache_path else None,
+                                C.byref(bp), _stream(stream)), "rq_autotune_batch")
+    return bp
+
+
+# ------------------------------------------------------------ serving ----
+
+class Server:
+    """Continuous-batching AO bake server (see rq_server_* in include/rq.h)."""
+
+    def __init__(self, hbm_budget_bytes: int, query: int = ANY, streams: int = 3, max_batch_rays: int = 0,
+                 launch: Optional[Launch] = None):
+        p = N.ServerParams(hbm_budget_bytes, max_batch_rays, streams, query,
+                           launch if launch is not None else Launch())
+        h = C.c_void_p()
+        check(lib.rq_server_create(C.byref(p), C.byref(h)), "rq_server_create")
+        self._h = h
+        self._scenes = []
+
+    def add_scene(self, scene: Scene) -> int:
+        sid = C.c_int32()
+        check(lib.rq_server_add_scene(self._h, scene._h, C.byref(sid)), "rq_server_add_scene")
+        self._scenes.append(scene)
+        return sid.value
+
+    def submit(self, scene_id: int, host_rays: np.ndarray, host_hits: np.ndarray) -> int:
+        """host_rays (n, 8) float32 and host_hits (n, 4) float32, kept alive by the caller until wait()."""
+        t = C.c_uint64()
+        n = host_rays.size // 8
+        check(lib.rq_server_submit(self._h, scene_id, host_rays.ctypes.data, host_hits.ctypes.data, n, C.byref(t)),
+              "rq_server_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
+        st = N.RequestStats()
+        s = lib.rq_server_wait(self._h, ticket, timeout_ms, C.byref(st))
+        out = {f: getattr(st, f) for f, _ in N.RequestStats._fields_}
+        out["status_name"] = N.STATUS.get(s, str(s))
+        if s not in (0,):
+            raise RQError(s, "rq_server_wait")
+        return out
+
+    def cancel(self, ticket: int) -> int:
+        return int(lib.rq_server_cancel(self._h, ticket))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+# ------------------------------------------ reference-shaped entry points ----
+
+def rtBindCWBVHData(nodes, woop, prim_index=None) -> None:
+    check(lib.rq_rtBindCWBVHData(_ptr(nodes), _ptr(woop), _ptr(prim_index) or None), "rtBindCWBVHData")
+
+
+def rtTraceCWBVH(rays, hits, ray_count: int) -> None:
+    check(lib.rq_rtTraceCWBVH(_ptr(rays), _ptr(hits), ray_count), "rtTraceCWBVH")
+
+
+def rtBindBVH2Data(nodes, woop, prim_index=None) -> None:
+    check(lib.rq_rtBindBVH2Data(_ptr(nodes), _ptr(woop), _ptr(prim_index) or None), "rtBindBVH2Data")
+
+
+def rtTraceBVH2(rays, hits, ray_count: int) -> None:
+    check(lib.rq_rtTraceBVH2(_ptr(rays), _ptr(hits), ray_count), "rtTraceBVH2")
+
+
+def rtOccludedCWBVH(rays, hits, ray_count: int) -> None:
+    check(lib.rq_rtOccludedCWBVH(_ptr(rays), _ptr(hits), ray_count), "rtOccludedCWBVH")
+
+
+def rtOccludedBVH2(rays, hits, ray_count: int) -> None:
+    check(lib.rq_rtOccludedBVH2(_ptr(rays), _ptr(hits), ray_count), "rtOccludedBVH2")
+
+
+def GenerateAORaysUniform(num_texels: int, rays_per_texel: int, pos: np.ndarray, nrm: np.ndarray,
+                          radius: np.ndarray):
+    """Host surfel arrays in, a torch CUDA tensor of rays out (tmin 0.01, tmax 1e20, offset radius/2)."""
+    import torch
+    pos = np.ascontiguousarray(pos, np.float32)
+    nrm = np.ascontiguousarray(nrm, np.float32)
+    radius = np.ascontiguousarray(radius, np.float32)
+    p = lib.rq_GenerateAORaysUniform(num_texels, rays_per_texel, pos.ctypes.data, nrm.ctypes.data,
+                                     radius.ctypes.data)
+    if not p:
+        raise RQError(5, "GenerateAORaysUniform")
+    n = num_texels * rays_per_texel
+    out = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+    try:
+        check(lib.rq_device_copy(out.data_ptr(), p, n * 32), "rq_device_copy")
+    finally:
+        lib.rq_device_free(p)
+    return out

@@ -1,0 +1,366 @@
+// Binned-SAH BVH builder.  It stands in for the reference's Embree build
+// (BuildBVH2Triangle / BuildBVH8Triangle, src/EmbreeBVHBuilder.cpp:303-478),
+// which is not available here.  A binary tree is built top-down with a binned
+// surface-area heuristic (object splits only; no spatial splits), then the
+// 8-wide tree for the CWBVH is made by greedily opening the largest-area inner
+// child until a node has 8 children.  Leaves of the 8-wide tree hold at most 3
+// triangles, as the reference asks Embree for (maxLeafSize = 3,
+// src/EmbreeBVHBuilder.cpp:456-457).
+//
+// Speed: primitive records (box + id, 32 B) are moved by the partition, so
+// every pass is sequential; one pass bins all three axes and records each
+// bin's box and centroid box, from which the children's bounds follow without
+// another pass; subtrees above a size threshold are built on other threads.
+#include <algorithm>
+#include <atomic>
+#include <future>
+#include <thread>
+
+#include "host_common.h"
+
+namespace rq {
+namespace {
+
+constexpr int kMaxBins = 64;
+constexpr float kTraversalCost = 1.0f;
+constexpr float kIntersectCost = 1.0f;
+constexpr int64_t kParallelGrain = 32768;
+
+struct alignas(32) PrimRef {
+    float lo[3];
+    int32_t id;
+    float hi[3];
+    int32_t pad;
+};
+
+// Plain min/max (inputs are finite); compiles to minss/maxss.
+inline float fmn(float a, float b) { return a < b ? a : b; }
+inline float fmx(float a, float b) { return a > b ? a : b; }
+
+struct BBox {
+    float lo[3] = {INFINITY, INFINITY, INFINITY};
+    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    void grow(const float* l, const float* h) {
+        for (int a = 0; a < 3; ++a) { lo[a] = fmn(lo[a], l[a]); hi[a] = fmx(hi[a], h[a]); }
+    }
+    void grow_pt(const float* p) { grow(p, p); }
+    void grow(const BBox& b) { grow(b.lo, b.hi); }
+    float area() const {
+        const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        if (!(dx >= 0.f && dy >= 0.f && dz >= 0.f)) return 0.f;
+        return 2.f * (dx * dy + dy * dz + dz * dx);
+    }
+};
+
+struct Bin {
+    BBox box, cbox;
+    int count = 0;
+};
+
+inline void centroid(const PrimRef& p, float c[3]) {
+    for (int a = 0; a < 3; ++a) c[a] = (p.lo[a] + p.hi[a]) * 0.5f;
+}
+
+struct Builder2 {
+    int max_leaf, bins, max_depth;
+    bool big_leaves;  // at the depth cap: one oversized leaf (BVH2) or median splits (CWBVH source)
+    std::vector<PrimRef> refs;
+    std::vector<TreeNode<2>> nodes;
+    std::vector<Leaf> leaves;
+    std::atomic<int32_t> n_nodes{0};
+    std::atomic<int32_t> n_leaves{0};
+    std::atomic<int> spare_threads{0};
+
+    int32_t make_leaf(int64_t begin, int64_t end) {
+        const int32_t l = n_leaves.fetch_add(1);
+        leaves[l] = Leaf{(int32_t)begin, (int32_t)(end - begin)};
+        return -(l + 2);
+    }
+
+    // Child code of the subtree over refs[begin, end) with bounds `b` and
+    // centroid bounds `cb`.
+    int32_t build(int64_t begin, int64_t end, const BBox& b, const BBox& cb, int depth) {
+        const int64_t n = end - begin;
+        const bool may_leaf = n <= max_leaf;
+        if (n == 1 || (depth >= max_depth && (may_leaf || big_leaves))) return make_leaf(begin, end);
+        if (depth >= max_depth) return median_split(begin, end, cb, depth);
+
+        // One pass: bin all three axes (fewer bins for small nodes: the bin
+        // arrays are initialised per node).
+        const int nb = (int)std::min<int64_t>(bins, std::max<int64_t>(4, n));
+        float scale[3];
+        bool usable[3];
+        for (int a = 0; a < 3; ++a) {
+            const float ext = cb.hi[a] - cb.lo[a];
+            usable[a] = ext > 0.f;
+            scale[a] = usable[a] ? (float)nb / ext : 0.f;
+        }
+        alignas(Bin) unsigned char storage[3 * kMaxBins * sizeof(Bin)];
+        Bin(*bin)[kMaxBins] = reinterpret_cast<Bin(*)[kMaxBins]>(storage);
+        for (int a = 0; a < 3; ++a)
+            for (int i = 0; i < nb; ++i) new (&bin[a][i]) Bin();
+        for (int64_t k = begin; k < end; ++k) {
+            const PrimRef& p = refs[k];
+            float c[3];
+            centroid(p, c);
+            for (int a = 0; a < 3; ++a) {
+                int bi = (int)((c[a] - cb.lo[a]) * scale[a]);
+                bi = bi < 0 ? 0 : (bi >= nb ? nb - 1 : bi);
+                Bin& x = bin[a][bi];
+                x.count++;
+                x.box.grow(p.lo, p.hi);
+                x.cbox.grow_pt(c);
+            }
+        }
+        float best_cost = INFINITY;
+        int best_axis = -1, best_bin = -1;
+        for (int a = 0; a < 3; ++a) {
+            if (!usable[a]) continue;
+            float right_area[kMaxBins];
+            int right_count[kMaxBins];
+            BBox rb;
+            int rc = 0;
+            for (int i = nb - 1; i > 0; --i) {
+                rb.grow(bin[a][i].box);
+                rc += bin[a][i].count;
+                right_area[i] = rb.area();
+                right_count[i] = rc;
+            }
+            BBox lb;
+            int lc = 0;
+            for (int i = 0; i < nb - 1; ++i) {
+                lb.grow(bin[a][i].box);
+                lc += bin[a][i].count;
+                if (lc == 0 || right_count[i + 1] == 0) continue;
+                const float c = lb.area() * lc + right_area[i + 1] * right_count[i + 1];
+                if (c < best_cost) { best_cost = c; best_axis = a; best_bin = i; }
+            }
+        }
+        const float parent_area = b.area();
+        const float split_cost =
+            kTraversalCost + kIntersectCost * (parent_area > 0.f ? best_cost / parent_area : 0.f);
+        if (may_leaf && (best_axis < 0 || kIntersectCost * (float)n <= split_cost)) return make_leaf(begin, end);
+        if (best_axis < 0) return median_split(begin, end, cb, depth);  // all centroids coincide
+
+        const int a = best_axis;
+        const float lo = cb.lo[a], sc = scale[a];
+        PrimRef* first = refs.data() + begin;
+        PrimRef* m = std::partition(first, refs.data() + end, [&](const PrimRef& p) {
+            int bi = (int)(((p.lo[a] + p.hi[a]) * 0.5f - lo) * sc);
+            bi = bi < 0 ? 0 : (bi >= nb ? nb - 1 : bi);
+            return bi <= best_bin;
+        });
+        const int64_t mid = begin + (m - first);
+        if (mid == begin || mid == end) return median_split(begin, end, cb, depth);
+        BBox lb, lcb, rb, rcb;
+        for (int i = 0; i < nb; ++i) {
+            if (i <= best_bin) { lb.grow(bin[a][i].box); lcb.grow(bin[a][i].cbox); }
+            else { rb.grow(bin[a][i].box); rcb.grow(bin[a][i].cbox); }
+        }
+        return make_inner(begin, mid, end, lb, lcb, rb, rcb, depth);
+    }
+
+    // Balanced split at the centroid median of the widest centroid axis; keeps
+    // the depth bounded by log2(n) once the SAH recursion reaches the cap.
+    int32_t median_split(int64_t begin, int64_t end, const BBox& cb, int depth) {
+        int axis = 0;
+        float widest = -1.f;
+        for (int a = 0; a < 3; ++a)
+            if (cb.hi[a] - cb.lo[a] > widest) { widest = cb.hi[a] - cb.lo[a]; axis = a; }
+        const int64_t mid = begin + (end - begin) / 2;
+        std::nth_element(refs.data() + begin, refs.data() + mid, refs.data() + end,
+                         [&](const PrimRef& x, const PrimRef& y) {
+                             return x.lo[axis] + x.hi[axis] < y.lo[axis] + y.hi[axis];
+                         });
+        BBox lb, lcb, rb, rcb;
+        for (int64_t k = begin; k < end; ++k) {
+            float c[3];
+            centroid(refs[k], c);
+            if (k < mid) { lb.grow(refs[k].lo, refs[k].hi); lcb.grow_pt(c); }
+            else { rb.grow(refs[k].lo, refs[k].hi); rcb.grow_pt(c); }
+        }
+        return make_inner(begin, mid, end, lb, lcb, rb, rcb, depth);
+    }
+
+    int32_t make_inner(int64_t begin, int64_t mid, int64_t end, const BBox& lb, const BBox& lcb, const BBox& rb,
+                       const BBox& rcb, int depth) {
+        const int64_t n = end - begin;
+        const int32_t me = n_nodes.fetch_add(1);
+        int32_t lc, rc;
+        bool spawned = false;
+        std::future<int32_t> fut;
+        if (n > kParallelGrain) {
+            if (spare_threads.fetch_sub(1) > 0) {
+                spawned = true;
+                fut = std::async(std::launch::async, [=, this] { return build(begin, mid, lb, lcb, depth + 1); });
+            } else {
+                spare_threads.fetch_add(1);
+            }
+        }
+        if (spawned) {
+            rc = build(mid, end, rb, rcb, depth + 1);
+            lc = fut.get();
+            spare_threads.fetch_add(1);
+        } else {
+            lc = build(begin, mid, lb, lcb, depth + 1);
+            rc = build(mid, end, rb, rcb, depth + 1);
+        }
+        TreeNode<2> node{};
+        node.count = 2;
+        node.child[0] = lc;
+        node.child[1] = rc;
+        for (int a = 0; a < 3; ++a) {
+            node.lo[0][a] = lb.lo[a]; node.hi[0][a] = lb.hi[a];
+            node.lo[1][a] = rb.lo[a]; node.hi[1][a] = rb.hi[a];
+        }
+        nodes[me] = node;
+        return me;
+    }
+};
+
+}  // namespace
+
+void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
+                     Tree<2>& out) {
+    Builder2 b;
+    const int64_t nt = m.nt();
+    b.max_leaf = max_leaf;
+    b.big_leaves = big_leaves;
+    b.bins = std::max(2, std::min(bins, kMaxBins));
+    b.max_depth = max_depth;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    b.spare_threads = threads - 1;
+    b.refs.resize(nt);
+    BBox all, call;
+    for (int64_t t = 0; t < nt; ++t) {
+        PrimRef& p = b.refs[t];
+        for (int a = 0; a < 3; ++a) { p.lo[a] = INFINITY; p.hi[a] = -INFINITY; }
+        for (int k = 0; k < 3; ++k) {
+            const float* v = &m.v[3 * (size_t)m.i[3 * t + k]];
+            for (int a = 0; a < 3; ++a) { p.lo[a] = fmn(p.lo[a], v[a]); p.hi[a] = fmx(p.hi[a], v[a]); }
+        }
+        p.id = (int32_t)t;
+        p.pad = 0;
+        float c[3];
+        centroid(p, c);
+        all.grow(p.lo, p.hi);
+        call.grow_pt(c);
+    }
+    b.nodes.resize(std::max<int64_t>(1, 2 * nt));
+    b.leaves.resize(std::max<int64_t>(1, nt));
+
+    out = Tree<2>();
+    out.bounds.lo = v3(all.lo[0], all.lo[1], all.lo[2]);
+    out.bounds.hi = v3(all.hi[0], all.hi[1], all.hi[2]);
+    if (nt == 0) {
+        out.root_is_leaf = true;
+        out.leaves.push_back(Leaf{0, 0});
+        return;
+    }
+    const int32_t root = b.build(0, nt, all, call, 0);
+    out.prim_refs.resize(nt);
+    for (int64_t t = 0; t < nt; ++t) out.prim_refs[t] = b.refs[t].id;
+    if (root < 0) {
+        out.root_is_leaf = true;
+        out.leaves.push_back(b.leaves[-root - 2]);
+        return;
+    }
+    // Slots are handed out in parallel; the root took slot 0.
+    b.nodes.resize(b.n_nodes.load());
+    b.leaves.resize(b.n_leaves.load());
+    out.nodes = std::move(b.nodes);
+    out.leaves = std::move(b.leaves);
+}
+
+void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out) {
+    out = Tree<8>();
+    out.bounds = t2.bounds;
+    out.prim_refs = t2.prim_refs;
+    out.leaves = t2.leaves;
+    if (t2.root_is_leaf) {
+        // A single-leaf scene becomes an inner root with one leaf child.
+        TreeNode<8> r{};
+        for (int k = 0; k < 8; ++k) r.child[k] = -1;
+        const bool empty = t2.leaves.empty() || t2.leaves[0].count == 0;
+        r.count = empty ? 0 : 1;
+        r.child[0] = empty ? -1 : -2;
+        r.lo[0][0] = t2.bounds.lo.x; r.lo[0][1] = t2.bounds.lo.y; r.lo[0][2] = t2.bounds.lo.z;
+        r.hi[0][0] = t2.bounds.hi.x; r.hi[0][1] = t2.bounds.hi.y; r.hi[0][2] = t2.bounds.hi.z;
+        out.nodes.push_back(r);
+        return;
+    }
+    struct Item { int32_t src; int32_t dst; };
+    std::vector<Item> work;
+    out.nodes.reserve(t2.nodes.size() / 3 + 1);
+    out.nodes.push_back(TreeNode<8>{});
+    work.push_back({0, 0});
+    while (!work.empty()) {
+        const Item it = work.back();
+        work.pop_back();
+        const TreeNode<2>& s = t2.nodes[it.src];
+        int32_t code[8];
+        float lo[8][3], hi[8][3];
+        int cnt = 2;
+        for (int c = 0; c < 2; ++c) {
+            code[c] = s.child[c];
+            for (int a = 0; a < 3; ++a) { lo[c][a] = s.lo[c][a]; hi[c][a] = s.hi[c][a]; }
+        }
+        while (cnt < 8) {
+            int pick = -1;
+            float best = -1.f;
+            for (int c = 0; c < cnt; ++c) {
+                if (code[c] < 0) continue;
+                BBox b;
+                for (int a = 0; a < 3; ++a) { b.lo[a] = lo[c][a]; b.hi[a] = hi[c][a]; }
+                const float ar = b.area();
+                if (ar > best) { best = ar; pick = c; }
+            }
+            if (pick < 0) break;
+            const TreeNode<2>& o = t2.nodes[code[pick]];
+            code[pick] = o.child[0];
+            code[cnt] = o.child[1];
+            for (int a = 0; a < 3; ++a) {
+                lo[pick][a] = o.lo[0][a]; hi[pick][a] = o.hi[0][a];
+                lo[cnt][a] = o.lo[1][a];  hi[cnt][a] = o.hi[1][a];
+            }
+            ++cnt;
+        }
+        TreeNode<8> d{};
+        d.count = cnt;
+        for (int k = 0; k < 8; ++k) d.child[k] = -1;
+        for (int c = 0; c < cnt; ++c) {
+            for (int a = 0; a < 3; ++a) { d.lo[c][a] = lo[c][a]; d.hi[c][a] = hi[c][a]; }
+            if (code[c] < 0) {
+                d.child[c] = code[c];
+            } else {
+                const int32_t ni = (int32_t)out.nodes.size();
+                out.nodes.push_back(TreeNode<8>{});
+                d.child[c] = ni;
+                work.push_back({code[c], ni});
+            }
+        }
+        out.nodes[it.dst] = d;
+    }
+}
+
+template <int W>
+static int depth_of(const Tree<W>& t) {
+    if (t.root_is_leaf || t.nodes.empty()) return 1;
+    std::vector<std::pair<int32_t, int>> st{{0, 1}};
+    int best = 1;
+    while (!st.empty()) {
+        auto [n, d] = st.back();
+        st.pop_back();
+        const auto& nd = t.nodes[n];
+        for (int c = 0; c < W; ++c) {
+            if (nd.child[c] >= 0) st.push_back({nd.child[c], d + 1});
+            else if (nd.child[c] <= -2) best = std::max(best, d + 1);
+        }
+    }
+    return best;
+}
+
+int tree_depth2(const Tree<2>& t) { return depth_of(t); }
+int tree_depth8(const Tree<8>& t) { return depth_of(t); }
+
+}  // namespace rq

@@ -1,0 +1,460 @@
+// Persistent trace kernels for sm_100a: the compressed 8-wide BVH (CWBVH) and
+// the binary BVH (BVH2), closest-hit and any-hit, over one scene or over a
+// batch of (scene, rays) items in one launch.
+//
+// Work distribution (both kernels).  One CTA per SM slot stays resident for the
+// whole launch.  A warp hands rays to its idle lanes from one 64-bit global
+// counter: the lanes that need a ray vote, one lane adds their count to the
+// counter and broadcasts the old value (the reference's per-warp atomicAdd,
+// src/TraversalKernelCWBVH.cu:56-87, written with __shfl_sync instead of a
+// volatile shared word so it is correct under independent thread scheduling).
+// A warp re-fills after the idle lanes have cost Nw lane-iterations beyond Nd
+// (src/TraversalKernelCWBVH.cu:365-371).  Every vote is over the full warp and
+// every loop is warp-uniform, so lanes never diverge around a collective.
+//
+// Safety.  A ray whose stack would overflow, whose node/triangle index falls
+// outside the buffers, or that runs more than kStepLimit steps is finished as
+// a miss and the context's error word records why; the kernel itself never
+// reads outside the buffers it was given and never spins without a bound.
+#include <cstdio>
+
+#include "device_api.h"
+#include "trace_common.cuh"
+
+namespace rq {
+
+constexpr int kStackTotal = 64;  // entries per lane (shared + local)
+constexpr uint32_t kBvh2Sentinel = 0x76543210u;  // src/TraversalKernelBVH2.cu:33
+
+// Resolves a global ray index to its item (batch) and loads the ray.
+struct Lane {
+    const float4* nodes;
+    const float4* woop;
+    Hit* hits;
+    int64_t out_idx;
+    int64_t gidx;
+    uint32_t node_f4, woop_f4;
+};
+
+template <bool MULTI>
+__device__ __forceinline__ Ray fetch_ray(const TraceParams& p, int64_t g, Lane& L) {
+    const TraceItem* it = &p.single;
+    if (MULTI) {
+        int lo = 0, hi = p.n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (p.items[mid].ray_begin <= g) lo = mid; else hi = mid - 1;
+        }
+        it = p.items + lo;
+    }
+    const int64_t local = g - (MULTI ? it->ray_begin : 0);
+    L.nodes = it->nodes;
+    L.woop = it->woop;
+    L.hits = it->hits;
+    L.node_f4 = it->node_f4;
+    L.woop_f4 = it->woop_f4;
+    L.out_idx = it->perm ? (int64_t)__ldg(it->perm + local) : local;
+    L.gidx = g;
+    Ray r;
+    r.origin_tmin = __ldcs(&it->rays[local].origin_tmin);
+    r.dir_tmax = __ldcs(&it->rays[local].dir_tmax);
+    return r;
+}
+
+__device__ __forceinline__ void store_hit(Hit* hits, int64_t i, float t, int addr, float u, float v) {
+    __stcs(&hits[i].t_triId_u_v, make_float4(t, __int_as_float(addr), u, v));
+}
+
+// ------------------------------------------------------------------ CWBVH --
+
+template <bool ANY, int SMEM, bool MULTI, bool COUNT>
+__global__ void __launch_bounds__(512) cwbvh_kernel(const TraceParams p) {
+    extern __shared__ uint2 sstack[];
+    constexpr int LOCAL = kStackTotal - SMEM;
+    uint2 lstack[LOCAL];
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned tid = threadIdx.x;
+    const unsigned B = blockDim.x;
+
+    Lane L{};
+    float ox = 0.f, oy = 0.f, oz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f, tmin = 0.f, tmax = 0.f;
+    float idx_ = 0.f, idy = 0.f, idz = 0.f;
+    unsigned octinv = 0, octinv4 = 0;
+    uint2 ng = make_uint2(0u, 0u), tg = make_uint2(0u, 0u);
+    int sp = 0, hit_addr = -1, steps = 0, nvis = 0, ntri = 0;
+    float hu = 0.f, hv = 0.f;
+    bool active = false, exhausted = false;
+    const float rt = p.postpone_ratio;
+
+    auto push = [&](uint2 v) -> bool {
+        if (sp < SMEM) sstack[(unsigned)sp * B + tid] = v;
+        else if (sp < kStackTotal) lstack[sp - SMEM] = v;
+        else return false;
+        ++sp;
+        return true;
+    };
+    auto pop = [&]() -> uint2 {
+        --sp;
+        return sp < SMEM ? sstack[(unsigned)sp * B + tid] : lstack[sp - SMEM];
+    };
+    auto finish = [&](unsigned err) {
+        if (err) {
+            atomicOr(&p.scratch->error, err);
+            hit_addr = -1;
+        }
+        store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
+        if (COUNT) {
+            p.node_visits[L.gidx] = nvis;
+            p.tri_tests[L.gidx] = ntri;
+        }
+        active = false;
+    };
+
+    for (;;) {
+        // ---- hand rays to idle lanes
+        const bool need = !active && !exhausted;
+        const unsigned needm = __ballot_sync(kFullMask, need);
+        if (needm) {
+            const int leader = __ffs(needm) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&p.scratch->ray_counter, (unsigned long long)__popc(needm));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (need) {
+                const int64_t g = (int64_t)base + __popc(needm & lanemask_lt());
+                if (g < p.total_rays) {
+                    const Ray r = fetch_ray<MULTI>(p, g, L);
+                    ox = r.origin_tmin.x; oy = r.origin_tmin.y; oz = r.origin_tmin.z; tmin = r.origin_tmin.w;
+                    dx = r.dir_tmax.x; dy = r.dir_tmax.y; dz = r.dir_tmax.z; tmax = r.dir_tmax.w;
+                    idx_ = guarded_rcp(dx);
+                    idy = guarded_rcp(dy);
+                    idz = guarded_rcp(dz);
+                    octinv = 7u - (((dx < 0.f) ? 4u : 0u) | ((dy < 0.f) ? 2u : 0u) | ((dz < 0.f) ? 1u : 0u));
+                    octinv4 = octinv * 0x01010101u;
+                    ng = make_uint2(0u, 0x80000000u);
+                    tg = make_uint2(0u, 0u);
+                    sp = 0; hit_addr = -1; hu = 0.f; hv = 0.f; steps = 0; nvis = 0; ntri = 0;
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (__ballot_sync(kFullMask, active) == 0u) break;
+
+        int lost = 0;
+        for (;;) {
+            // ---- node phase: take the nearest child of the current node group
+            unsigned fault = 0u;
+            if (active) {
+                if (ng.y > 0x00FFFFFFu) {
+                    const unsigned hitsm = ng.y;
+                    const unsigned bit = highest_bit(hitsm);
+                    const unsigned base = ng.x;
+                    ng.y &= ~(1u << bit);
+                    if (ng.y > 0x00FFFFFFu && !push(ng)) fault = kErrStackOverflow;
+                    const unsigned slot = (bit - 24u) ^ octinv;
+                    const unsigned ci = base + (unsigned)__popc(hitsm & ~(0xFFFFFFFFu << slot));
+                    if (++steps > kStepLimit) fault |= kErrTimeout;
+                    if ((uint64_t)ci * 5u + 5u > (uint64_t)L.node_f4) fault |= kErrBadScene;
+                    if (!fault) {
+                        const float4* np = L.nodes + (size_t)ci * 5u;
+                        const float4 n0 = ld_nc(np + 0), n1 = ld_nc(np + 1), n2 = ld_nc(np + 2);
+                        const float4 n3 = ld_nc(np + 3), n4 = ld_nc(np + 4);
+                        if (COUNT) ++nvis;
+                        const unsigned ew = __float_as_uint(n0.w);
+                        const float adjx = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)(ew & 0xFFu) + 127)) << 23), idx_);
+                        const float adjy = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)((ew >> 8) & 0xFFu) + 127)) << 23), idy);
+                        const float adjz = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)((ew >> 16) & 0xFFu) + 127)) << 23), idz);
+                        const float orx = __fmul_rn(-__fsub_rn(ox, n0.x), idx_);
+                        const float ory = __fmul_rn(-__fsub_rn(oy, n0.y), idy);
+                        const float orz = __fmul_rn(-__fsub_rn(oz, n0.z), idz);
+                        unsigned hitmask = 0u;
+#pragma unroll
+                        for (int g = 0; g < 2; ++g) {
+                            const unsigned meta4 = __float_as_uint(g == 0 ? n1.z : n1.w);
+                            const unsigned inner4 = ((meta4 & (meta4 << 1)) & 0x10101010u) >> 4;
+                            const unsigned bitidx4 = (meta4 ^ (octinv4 & (inner4 * 0xFFu))) & 0x1F1F1F1Fu;
+                            const unsigned bits4 = (meta4 >> 5) & 0x07070707u;
+                            const unsigned wlx = __float_as_uint(g == 0 ? n2.x : n2.y);
+                            const unsigned whx = __float_as_uint(g == 0 ? n3.z : n3.w);
+                            const unsigned wly = __float_as_uint(g == 0 ? n2.z : n2.w);
+                            const unsigned why = __float_as_uint(g == 0 ? n4.x : n4.y);
+                            const unsigned wlz = __float_as_uint(g == 0 ? n3.x : n3.y);
+                            const unsigned whz = __float_as_uint(g == 0 ? n4.z : n4.w);
+                            const unsigned lox = idx_ < 0.f ? whx : wlx, hix = idx_ < 0.f ? wlx : whx;
+                            const unsigned loy = idy < 0.f ? why : wly, hiy = idy < 0.f ? wly : why;
+                            const unsigned loz = idz < 0.f ? whz : wlz, hiz = idz < 0.f ? wlz : whz;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) {
+                                const float tx0 = __fmaf_rn(byte_to_float(lox, c), adjx, orx);
+                                const float ty0 = __fmaf_rn(byte_to_float(loy, c), adjy, ory);
+                                const float tz0 = __fmaf_rn(byte_to_float(loz, c), adjz, orz);
+                                const float tx1 = __fmaf_rn(byte_to_float(hix, c), adjx, orx);
+                                const float ty1 = __fmaf_rn(byte_to_float(hiy, c), adjy, ory);
+                                const float tz1 = __fmaf_rn(byte_to_float(hiz, c), adjz, orz);
+                                const float cmin = fmaxf(imax3(tx0, ty0, tz0), tmin);
+                                const float cmax = fminf(imin3(tx1, ty1, tz1), tmax);
+                                if (cmin <= cmax)
+                                    hitmask |= ((bits4 >> (8 * c)) & 0xFFu) << ((bitidx4 >> (8 * c)) & 0xFFu);
+                            }
+                        }
+                        ng = make_uint2(__float_as_uint(n1.x), (hitmask & 0xFF000000u) | (ew >> 24));
+                        tg = make_uint2(__float_as_uint(n1.y), hitmask & 0x00FFFFFFu);
+                    }
+                } else {
+                    tg = ng;
+                    ng = make_uint2(0u, 0u);
+                }
+                if (fault) finish(fault);
+            }
+
+            // ---- triangle phase, warp-synchronous; postpone when few lanes remain
+            {
+                const int total = __popc(__ballot_sync(kFullMask, active));
+                const int threshold = (int)((float)total * rt);
+                for (;;) {
+                    const bool want = active && tg.y != 0u;
+                    const unsigned wm = __ballot_sync(kFullMask, want);
+                    if (wm == 0u) break;
+                    if (__popc(wm) < threshold) {
+                        if (want && !push(tg)) finish(kErrStackOverflow);
+                        break;
+                    }
+                    if (want) {
+                        const unsigned ti = highest_bit(tg.y);
+                        const unsigned tri = tg.x * 3u + ti * 3u;
+                        tg.y &= ~(1u << ti);
+                        if ((uint64_t)tri + 3u > (uint64_t)L.woop_f4) {
+                            finish(kErrBadScene);
+                        } else {
+                            const float4* tp = L.woop + tri;
+                            const float4 v0 = ld_nc(tp), v1 = ld_nc(tp + 1), v2 = ld_nc(tp + 2);
+                            if (COUNT) ++ntri;
+                            float t, u, v;
+                            if (woop_test(v0, v1, v2, ox, oy, oz, dx, dy, dz, tmin, tmax, t, u, v)) {
+                                tmax = t;
+                                hit_addr = (int)tri;
+                                hu = u;
+                                hv = v;
+                                if (ANY) finish(0u);
+                            }
+                        }
+                    }
+                }
+            }
+
+            // ---- continue with the stack, or finish the ray
+            if (active && ng.y <= 0x00FFFFFFu) {
+                if (sp > 0) ng = pop();
+                else finish(0u);
+            }
+
+            const unsigned am = __ballot_sync(kFullMask, active);
+            if (am == 0u) break;
+            lost += 32 - __popc(am) - p.fetch_nd;
+            if (lost >= p.fetch_nw) break;
+        }
+    }
+}
+
+// ------------------------------------------------------------------- BVH2 --
+
+template <bool ANY, int SMEM, bool MULTI, bool COUNT>
+__global__ void __launch_bounds__(512) bvh2_kernel(const TraceParams p) {
+    extern __shared__ int istack[];
+    constexpr int LOCAL = kStackTotal - SMEM;
+    int lstack[LOCAL];
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned tid = threadIdx.x;
+    const unsigned B = blockDim.x;
+    const bool speculate = p.bvh2_speculative != 0;
+
+    Lane L{};
+    float ox = 0.f, oy = 0.f, oz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f, tmin = 0.f, tmax = 0.f;
+    float idx_ = 0.f, idy = 0.f, idz = 0.f, oodx = 0.f, oody = 0.f, oodz = 0.f;
+    int node = 0, leaf = 0, tcur = 0, sp = 0, hit_addr = -1, steps = 0, nvis = 0, ntri = 0;
+    float hu = 0.f, hv = 0.f;
+    bool active = false, exhausted = false;
+
+    // Stack slot 0 holds the sentinel; entries 1.. are pushed far children.
+    auto push = [&](int v) -> bool {
+        ++sp;
+        if (sp < SMEM) istack[(unsigned)sp * B + tid] = v;
+        else if (sp < kStackTotal) lstack[sp - SMEM] = v;
+        else { --sp; return false; }
+        return true;
+    };
+    auto pop = [&]() -> int {
+        const int v = sp == 0 ? (int)kBvh2Sentinel : (sp < SMEM ? istack[(unsigned)sp * B + tid] : lstack[sp - SMEM]);
+        if (sp > 0) --sp;
+        return v;
+    };
+    auto finish = [&](unsigned err) {
+        if (err) {
+            atomicOr(&p.scratch->error, err);
+            hit_addr = -1;
+        }
+        store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
+        if (COUNT) {
+            p.node_visits[L.gidx] = nvis;
+            p.tri_tests[L.gidx] = ntri;
+        }
+        active = false;
+    };
+
+    for (;;) {
+        const bool need = !active && !exhausted;
+        const unsigned needm = __ballot_sync(kFullMask, need);
+        if (needm) {
+            const int leader = __ffs(needm) - 1;
+            unsigned long long base = 0;
+            if ((int)lane == leader) base = atomicAdd(&p.scratch->ray_counter, (unsigned long long)__popc(needm));
+            base = __shfl_sync(kFullMask, base, leader);
+            if (need) {
+                const int64_t g = (int64_t)base + __popc(needm & lanemask_lt());
+                if (g < p.total_rays) {
+                    const Ray r = fetch_ray<MULTI>(p, g, L);
+                    ox = r.origin_tmin.x; oy = r.origin_tmin.y; oz = r.origin_tmin.z; tmin = r.origin_tmin.w;
+                    dx = r.dir_tmax.x; dy = r.dir_tmax.y; dz = r.dir_tmax.z; tmax = r.dir_tmax.w;
+                    idx_ = guarded_rcp(dx);
+                    idy = guarded_rcp(dy);
+                    idz = guarded_rcp(dz);
+                    oodx = __fmul_rn(ox, idx_);
+                    oody = __fmul_rn(oy, idy);
+                    oodz = __fmul_rn(oz, idz);
+                    node = 0; leaf = 0; sp = 0; hit_addr = -1; hu = 0.f; hv = 0.f; steps = 0; nvis = 0; ntri = 0;
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (__ballot_sync(kFullMask, active) == 0u) break;
+
+        int lost = 0;
+        for (;;) {
+            // ---- inner-node loop (src/TraversalKernelBVH2.cu:70-122)
+            if (active) leaf = 0;
+            for (;;) {
+                const bool in = active && node != (int)kBvh2Sentinel && node >= 0 && (speculate || leaf >= 0);
+                if (__ballot_sync(kFullMask, in) == 0u) break;
+                if (in) {
+                    unsigned fault = 0u;
+                    if (++steps > kStepLimit) fault |= kErrTimeout;
+                    if ((uint64_t)(unsigned)node + 4u > (uint64_t)L.node_f4) fault |= kErrBadScene;
+                    if (!fault) {
+                        const float4* np = L.nodes + node;
+                        const float4 n0 = ld_nc(np), n1 = ld_nc(np + 1), n2 = ld_nc(np + 2), n3 = ld_nc(np + 3);
+                        if (COUNT) ++nvis;
+                        // Slabs: lo * idir - ood (src/TraversalKernelBVH2.cu:16-19).
+                        const float a0lx = __fmaf_rn(n0.x, idx_, -oodx), a0hx = __fmaf_rn(n0.y, idx_, -oodx);
+                        const float a0ly = __fmaf_rn(n0.z, idy, -oody), a0hy = __fmaf_rn(n0.w, idy, -oody);
+                        const float a0lz = __fmaf_rn(n2.x, idz, -oodz), a0hz = __fmaf_rn(n2.y, idz, -oodz);
+                        const float a1lx = __fmaf_rn(n1.x, idx_, -oodx), a1hx = __fmaf_rn(n1.y, idx_, -oodx);
+                        const float a1ly = __fmaf_rn(n1.z, idy, -oody), a1hy = __fmaf_rn(n1.w, idy, -oody);
+                        const float a1lz = __fmaf_rn(n2.z, idz, -oodz), a1hz = __fmaf_rn(n2.w, idz, -oodz);
+                        const float c0min = imin_then_max(a0lz, a0hz, imin_then_max(a0ly, a0hy, imin_then_max(a0lx, a0hx, tmin)));
+                        const float c0max = imax_then_min(a0lz, a0hz, imax_then_min(a0ly, a0hy, imax_then_min(a0lx, a0hx, tmax)));
+                        const float c1min = imin_then_max(a1lz, a1hz, imin_then_max(a1ly, a1hy, imin_then_max(a1lx, a1hx, tmin)));
+                        const float c1max = imax_then_min(a1lz, a1hz, imax_then_min(a1ly, a1hy, imax_then_min(a1lx, a1hx, tmax)));
+                        const bool t0 = c0min <= c0max, t1 = c1min <= c1max;
+                        int cx = __float_as_int(n3.x), cy = __float_as_int(n3.y);
+                        if (!t0 && !t1) {
+                            node = pop();
+                        } else {
+                            node = t0 ? cx : cy;
+                            if (t0 && t1) {
+                                if (c1min < c0min) { const int tmp = node; node = cy; cy = tmp; }
+                                if (!push(cy)) fault |= kErrStackOverflow;
+                            }
+                        }
+                        if (!fault && node < 0 && leaf >= 0) {
+                            leaf = node;
+                            node = pop();
+                        }
+                    }
+                    if (fault) finish(fault);
+                }
+                if (speculate && __ballot_sync(kFullMask, in && leaf >= 0) == 0u) break;
+            }
+
+            // ---- leaf loop, one triangle per iteration (src/TraversalKernelBVH2.cu:124-169)
+            if (active && leaf < 0) tcur = ~leaf;
+            for (;;) {
+                const bool want = active && leaf < 0;
+                if (__ballot_sync(kFullMask, want) == 0u) break;
+                if (want) {
+                    if ((uint64_t)(unsigned)tcur + 1u > (uint64_t)L.woop_f4) {
+                        finish(kErrBadScene);
+                    } else {
+                        const float4 v0 = ld_nc(L.woop + tcur);
+                        if (__float_as_uint(v0.x) == 0x80000000u) {
+                            // Leaf terminator: move to the postponed node / next leaf.
+                            leaf = node;
+                            if (node < 0) {
+                                node = pop();
+                                tcur = ~leaf;
+                            }
+                        } else if ((uint64_t)(unsigned)tcur + 3u > (uint64_t)L.woop_f4) {
+                            finish(kErrBadScene);
+                        } else {
+                            const float4 v1 = ld_nc(L.woop + tcur + 1), v2 = ld_nc(L.woop + tcur + 2);
+                            if (COUNT) ++ntri;
+                            float t, u, v;
+                            if (woop_test(v0, v1, v2, ox, oy, oz, dx, dy, dz, tmin, tmax, t, u, v)) {
+                                tmax = t;
+                                hit_addr = tcur;
+                                hu = u;
+                                hv = v;
+                                if (ANY) finish(0u);
+                            }
+                            tcur += 3;
+                        }
+                    }
+                }
+            }
+
+            if (active && node == (int)kBvh2Sentinel) finish(0u);
+
+            const unsigned am = __ballot_sync(kFullMask, active);
+            if (am == 0u) break;
+            lost += 32 - __popc(am) - p.fetch_nd;
+            if (lost >= p.fetch_nw) break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- launch --
+
+template <bool MULTI, bool COUNT>
+static TraceKernelFn select_cwbvh(bool any, int smem) {
+#define RQ_CW(A, S) (TraceKernelFn)cwbvh_kernel<A, S, MULTI, COUNT>
+    if (any) return smem <= 4 ? RQ_CW(true, 4) : (smem <= 8 ? RQ_CW(true, 8) : RQ_CW(true, 16));
+    return smem <= 4 ? RQ_CW(false, 4) : (smem <= 8 ? RQ_CW(false, 8) : RQ_CW(false, 16));
+#undef RQ_CW
+}
+template <bool MULTI, bool COUNT>
+static TraceKernelFn select_bvh2(bool any, int smem) {
+#define RQ_B2(A, S) (TraceKernelFn)bvh2_kernel<A, S, MULTI, COUNT>
+    if (any) return smem <= 4 ? RQ_B2(true, 4) : (smem <= 8 ? RQ_B2(true, 8) : RQ_B2(true, 16));
+    return smem <= 4 ? RQ_B2(false, 4) : (smem <= 8 ? RQ_B2(false, 8) : RQ_B2(false, 16));
+#undef RQ_B2
+}
+
+TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, bool count) {
+    if (kind == RQ_BVH_CWBVH) {
+        if (count) return select_cwbvh<false, true>(any, smem);
+        return multi ? select_cwbvh<true, false>(any, smem) : select_cwbvh<false, false>(any, smem);
+    }
+    if (count) return select_bvh2<false, true>(any, smem);
+    return multi ? select_bvh2<true, false>(any, smem) : select_bvh2<false, false>(any, smem);
+}
+
+int smem_entries_of(int requested) { return requested <= 4 ? 4 : (requested <= 8 ? 8 : 16); }
+
+size_t trace_smem_bytes(rq_bvh_kind kind, int smem_entries, int block) {
+    const size_t entry = kind == RQ_BVH_CWBVH ? sizeof(uint2) : sizeof(int);
+    return entry * (size_t)smem_entries * (size_t)block;
+}
+
+}  // namespace rq

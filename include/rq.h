@@ -1,0 +1,372 @@
+/*
+ * rq.h -- C ABI of the B200 ray-query engine (librq.so).
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns
+ * an rq_status (the reference aborts through cudaCheck/assert instead,
+ * src/CUDAAssert.h:5-12).  Device pointers are raw CUDA device addresses;
+ * streams are cudaStream_t handles passed as void*.
+ *
+ * Byte layouts kept from the reference (the drop-in contract):
+ *   Ray  = { float4 origin_tmin; float4 dir_tmax; }   32 B  (src/helper_math.h:1853-1857)
+ *   Hit  = { float4 t_triId_u_v; }                    16 B  (src/helper_math.h:1859-1865)
+ *          y holds the int bits of the Woop float4 address of the hit
+ *          triangle, or -1 for a miss.
+ *   CWBVH node = 5 x float4 = 80 B                    (src/GPUBVHConverter.cpp:141-145,310-375)
+ *   BVH2 node  = 4 x float4 = 64 B                    (src/GPUBVHConverter.cpp:69-72)
+ *   Woop triangle = 3 x float4 = 48 B                 (src/GPUBVHConverter.cpp:380-403)
+ *   BVH2 leaves end with a float4 whose x bits are 0x80000000
+ *                                                     (src/GPUBVHConverter.cpp:116-117)
+ */
+#ifndef RQ_H
+#define RQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+
+typedef enum rq_status {
+    RQ_OK = 0,
+    RQ_ERR_INVALID_ARG = 1,     /* null pointer, negative count, bad enum     */
+    RQ_ERR_OOM = 2,             /* device or host allocation failed          */
+    RQ_ERR_STACK_OVERFLOW = 3,  /* a ray needed more traversal stack entries  */
+    RQ_ERR_TIMEOUT = 4,         /* a ray exceeded its traversal step budget  */
+    RQ_ERR_CUDA = 5,            /* a CUDA runtime call failed                */
+    RQ_ERR_BAD_SCENE = 6,       /* a node/triangle index left the buffers    */
+    RQ_ERR_NOT_FOUND = 7,       /* unknown scene / request / ticket           */
+    RQ_ERR_BUDGET = 8,          /* request larger than the server HBM budget  */
+    RQ_ERR_CANCELLED = 9,       /* request cancelled or server shut down      */
+    RQ_ERR_NO_DEVICE = 10       /* no CUDA device visible                    */
+} rq_status;
+
+/* Human-readable name of a status code (static storage). */
+const char* rq_status_string(rq_status s);
+
+/* Text of the last CUDA error seen by this thread (static per-thread storage). */
+const char* rq_last_error(void);
+
+/* ------------------------------------------------------------------- types */
+
+typedef struct rq_ray { float origin_tmin[4]; float dir_tmax[4]; } rq_ray;
+typedef struct rq_hit { float t_triId_u_v[4]; } rq_hit;
+
+typedef enum rq_bvh_kind { RQ_BVH_CWBVH = 0, RQ_BVH_BVH2 = 1 } rq_bvh_kind;
+typedef enum rq_query { RQ_CLOSEST = 0, RQ_ANY = 1 } rq_query;
+
+/* Launch parameters of the persistent trace kernels.  Zero fields take the
+ * built-in defaults (or the autotuner's cached choice, see rq_autotune). */
+typedef struct rq_launch {
+    int block_size;       /* threads per block: 64, 128, 256 or 512             */
+    int blocks_per_sm;    /* persistent grid = SMs x this (0 = occupancy max)   */
+    int smem_stack;       /* stack entries per lane in shared memory: 4, 8, 16  */
+    float postpone_ratio; /* triangle postponing threshold Rt (reference 0.2)   */
+    int fetch_nd;         /* dynamic fetch: idle lanes tolerated (reference 4)  */
+    int fetch_nw;         /* dynamic fetch: lost-iteration budget (reference 16)*/
+} rq_launch;
+
+/* --------------------------------------------------- host BVH construction */
+/*
+ * A host BVH is the converter output of the reference: node buffer, Woop
+ * triangle buffer and the Woop-address -> primitive-index map, laid out
+ * byte-for-byte as ConvertToGPUBVH2 / ConvertToGPUCompressedWideBVH emit them
+ * (src/GPUBVHConverter.h:6-32).  The topology comes from this library's own
+ * binned-SAH builder, which replaces BuildBVH2Triangle / BuildBVH8Triangle
+ * (src/EmbreeBVHBuilder.h:39-43; Embree is not used).
+ */
+typedef struct rq_host_bvh* rq_host_bvh_t;
+
+typedef struct rq_build_params {
+    int max_leaf_size;    /* BVH2: max triangles per leaf (default 4); CWBVH is fixed at 3 */
+    int sah_bins;         /* binned-SAH bins per axis (default 32)                         */
+    int max_depth;        /* BVH2 depth limit (default 30; the reference stack is 32)      */
+    int threads;          /* builder threads (0 = hardware concurrency)                    */
+} rq_build_params;
+
+typedef struct rq_bvh_info {
+    int64_t node_float4s;     /* length of the node buffer in float4          */
+    int64_t woop_float4s;     /* length of the Woop buffer in float4          */
+    int64_t prim_index_count; /* length of the Woop-address -> primitive map  */
+    int64_t node_count;       /* nodes (80 B CWBVH / 64 B BVH2)              */
+    int64_t leaf_count;
+    int32_t depth;            /* levels from root to the deepest leaf          */
+    int32_t kind;             /* rq_bvh_kind                                   */
+    float bounds_lo[3];
+    float bounds_hi[3];
+} rq_bvh_info;
+
+/* Build a BVH over an indexed triangle mesh (vertices: 3*nv floats, indices:
+ * 3*nt ints) and convert it to the GPU layout of `kind`. */
+rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt,
+                       rq_bvh_kind kind, const rq_build_params* params, rq_host_bvh_t* out);
+rq_status rq_host_bvh_info(rq_host_bvh_t bvh, rq_bvh_info* out);
+/* Borrowed pointers into the host BVH (valid until rq_host_bvh_free). */
+rq_status rq_host_bvh_buffers(rq_host_bvh_t bvh, const float** nodes, const float** woop,
+                              const int32_t** prim_index);
+void rq_host_bvh_free(rq_host_bvh_t bvh);
+
+/* The builder's tree before conversion, for checking the converter against
+ * the reference's (src/GPUBVHConverter.cpp:10-378 consumes the same
+ * BVHNNode<N> shape, src/EmbreeBVHBuilder.h:7-37).  width is 2 (BVH2) or 8
+ * (CWBVH).  Per node: `width` child codes (>= 0 inner node, -1 empty slot,
+ * <= -2 leaf number -(code+2)) and `width` child boxes (lo xyz, hi xyz).
+ * Per leaf: first index into prim_refs and count.  Call with null arrays to
+ * get the sizes, then with arrays of those sizes. */
+rq_status rq_host_bvh_tree(rq_host_bvh_t bvh, int32_t* width, int64_t* n_nodes, int64_t* n_leaves,
+                           int64_t* n_prim_refs, int32_t* root_is_leaf, int32_t* child_codes,
+                           float* child_boxes, int32_t* leaf_first, int32_t* leaf_count,
+                           int32_t* prim_refs);
+
+/* Woop transform of one triangle: 3 float4 rows (V0, V1, V2) as
+ * WoopifyTriangle emits them (src/GPUBVHConverter.cpp:380-403). */
+rq_status rq_woopify(const float v0[3], const float v1[3], const float v2[3], float out_rows[12]);
+
+/* ----------------------------------------------------------- device scenes */
+typedef struct rq_scene* rq_scene_t;
+
+/* Register converted buffers as a device-resident scene.  With copy_from_host
+ * = 1 the buffers are host pointers and the scene owns device copies; with 0
+ * they are device pointers that the caller keeps alive (the reference's
+ * rtBind* ownership model, src/TraversalKernelCWBVH.cu:377-385). */
+rq_status rq_scene_create(rq_bvh_kind kind, const void* nodes, int64_t node_float4s,
+                          const void* woop, int64_t woop_float4s, const int32_t* prim_index,
+                          int64_t prim_index_count, int copy_from_host, rq_scene_t* out);
+/* Upload a host BVH (from rq_build_bvh) as a device scene. */
+rq_status rq_scene_from_host_bvh(rq_host_bvh_t bvh, rq_scene_t* out);
+rq_status rq_scene_destroy(rq_scene_t scene);
+rq_status rq_scene_device_buffers(rq_scene_t scene, const void** nodes, const void** woop,
+                                  const int32_t** prim_index);
+int64_t rq_scene_bytes(rq_scene_t scene);
+
+/* ---------------------------------------------------------------- contexts */
+/*
+ * A context owns the small device scratch of the persistent kernels (the
+ * dynamic-fetch ray counter and the error word).  Calls on one context are
+ * ordered by the stream they are given; use one context per concurrent stream.
+ */
+typedef struct rq_ctx* rq_ctx_t;
+
+rq_status rq_ctx_create(rq_ctx_t* out);
+rq_status rq_ctx_destroy(rq_ctx_t ctx);
+/* Wait for `stream`, read and clear the context's device error word. */
+rq_status rq_ctx_check(rq_ctx_t ctx, void* stream);
+
+/* ------------------------------------------------------------------ tracing */
+/*
+ * Trace `count` rays (device rq_ray[count]) into device rq_hit[count].
+ * RQ_CLOSEST follows rtTraceCWBVH / rtTraceBVH2 (src/TraversalKernelCWBVH.cu:387-426,
+ * src/TraversalKernelBVH2.cu:190-227): x = t of the closest hit (tmax on a
+ * miss), y = Woop address or -1, z/w = u,v of the hit.  RQ_ANY stops a ray at
+ * its first accepted triangle; only y != -1 (occluded) is contractual.
+ * Asynchronous on `stream`; errors detected by the kernel surface at rq_ctx_check.
+ */
+rq_status rq_trace(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,
+                   int64_t count, rq_query query, const rq_launch* launch, void* stream);
+
+/* Per-ray traversal counters (nodes fetched, triangles tested) written to
+ * device int32 arrays, for roofline accounting.  Traverses in the oracle's
+ * order (as rq_trace_ordered), so the counts match the CPU restatement's. */
+rq_status rq_trace_counted(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,
+                           int64_t count, rq_query query, int32_t* node_visits,
+                           int32_t* tri_tests, void* stream);
+
+/* rq_trace with the traversal order of the CPU oracle: no triangle
+ * postponing (CWBVH) and no speculative leaf postponing (BVH2).  Its results
+ * are bit-identical to the oracle's (t, id, u, v), which is what the parity
+ * tests check; rq_trace may differ from it only on exact ties. */
+rq_status rq_trace_ordered(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,
+                           int64_t count, rq_query query, void* stream);
+
+/* Defaults used when rq_launch fields are zero (a negative postpone_ratio
+ * turns triangle postponing off). */
+rq_status rq_default_launch(rq_bvh_kind kind, rq_query query, rq_launch* out);
+
+/* ------------------------------------------------------------ AO ray input */
+/*
+ * AO rays from a surfel sample cache, one ray per (surfel, sample): surfel
+ * s = i / spp, a cosine-weighted hemisphere direction about the surfel normal
+ * (concentric disk lifted to the hemisphere), origin = pos + n * radius *
+ * offset_scale, tmin/tmax as given.  Follows GenerateAORayUniformKernel
+ * (src/ValidationKernels.cu:41-101); the random numbers come from a
+ * Philox4x32-10 counter generator keyed by (seed, i) instead of curand XORWOW.
+ * pos/nrm are device float4[n_surfels], radius device float[n_surfels].
+ */
+rq_status rq_aorays(const float* pos, const float* nrm, const float* radius, int64_t n_surfels,
+                    int spp, uint64_t seed, float tmin, float tmax, float offset_scale,
+                    rq_ray* out_rays, void* stream);
+
+/* Surfels at uniformly chosen triangles (by index) and uniform barycentric
+ * points (square-root warp), geometric normals, radius 0.  vertices device
+ * float[3*nv], indices device int[3*nt]; outputs device float4/float4/float. */
+rq_status rq_sample_surfels(const float* vertices, const int32_t* indices, int64_t nt,
+                            int64_t n_surfels, uint64_t seed, float* out_pos, float* out_nrm,
+                            float* out_radius, void* stream);
+
+/* Per-surfel AO fraction (occluded rays / spp) from any-hit results whose rays
+ * were generated surfel-major (ray i belongs to surfel i / spp). */
+rq_status rq_ao_reduce(const rq_hit* hits, int64_t n_surfels, int spp, float* out_ao,
+                       void* stream);
+
+/* ---------------------------------------------------------- Morton sorting */
+/* Sort rays by a 32-bit key (10-bit Morton per origin axis inside the given
+ * bounds, high bits; direction octant, low bits).  Writes the sorted rays and
+ * the permutation (sorted position -> original index). */
+rq_status rq_sort_rays(rq_ctx_t ctx, const rq_ray* rays, int64_t count, const float bounds_lo[3],
+                       const float bounds_hi[3], rq_ray* sorted_rays, int32_t* perm,
+                       void* stream);
+
+/* -------------------------------------------------------------- batching */
+/*
+ * A batch traces many (scene, rays, hits) items in one persistent launch over
+ * device-resident scenes.  Rays of each item may be Morton-sorted first (items
+ * with at least sort_threshold rays); results land at the original ray index.
+ * rq_batch_run can be captured into a CUDA graph (use_graph = 1 replays one).
+ */
+typedef struct rq_batch* rq_batch_t;
+
+typedef struct rq_batch_item {
+    rq_scene_t scene;
+    const rq_ray* rays;   /* device */
+    rq_hit* hits;         /* device */
+    int64_t count;
+} rq_batch_item;
+
+typedef struct rq_batch_params {
+    rq_launch launch;
+    int64_t sort_threshold;  /* sort an item's rays when count >= this; <0 never */
+    int use_graph;           /* capture the launch sequence in a CUDA graph       */
+} rq_batch_params;
+
+rq_status rq_batch_create(rq_ctx_t ctx, const rq_batch_item* items, int n_items, rq_query query,
+                          const rq_batch_params* params, rq_batch_t* out);
+rq_status rq_batch_run(rq_batch_t batch, void* stream);
+/* One stage of rq_batch_run, eagerly (no graph): 1 = Morton sort of the
+ * sorted items' rays, 2 = the trace launch alone (reads the rays the last
+ * sort left).  Used to time the stages separately. */
+rq_status rq_batch_run_stage(rq_batch_t batch, int stage, void* stream);
+/* Kernels one rq_batch_run launches (counted from its captured graph when
+ * use_graph is set, else from the stages it runs). */
+int rq_batch_kernel_count(rq_batch_t batch);
+int64_t rq_batch_total_rays(rq_batch_t batch);
+rq_status rq_batch_destroy(rq_batch_t batch);
+
+/* ---------------------------------------------------------------- autotune */
+/*
+ * Time the candidate launch shapes (block size, blocks per SM, shared-memory
+ * stack depth, postponing ratio) on the given rays and return the fastest.
+ * When cache_path is non-null the choice is stored there keyed by device,
+ * BVH kind, query and size class, and later calls read it back.
+ */
+rq_status rq_autotune(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,
+                      int64_t count, rq_query query, const char* cache_path, rq_launch* out,
+                      void* stream);
+
+/* Tune a whole batch: sort threshold (never / large items / all) x block size
+ * x shared-memory stack depth, timed on the batch itself, cached like
+ * rq_autotune.  use_graph is set when `stream` is not the default stream. */
+rq_status rq_autotune_batch(rq_ctx_t ctx, const rq_batch_item* items, int n_items, rq_query query,
+                            const char* cache_path, rq_batch_params* out, void* stream);
+
+/* ----------------------------------------------------------------- serving */
+/*
+ * A continuous-batching AO bake server.  Requests (scene, host rays) are
+ * admitted while their ray/hit buffers fit the HBM budget, gathered into
+ * persistent batch launches on several streams (so batches overlap on the
+ * device), and completed by copying hits back to the caller's host buffer.
+ */
+typedef struct rq_server* rq_server_t;
+
+typedef struct rq_server_params {
+    int64_t hbm_budget_bytes;   /* ray+hit bytes admitted at once (48 B per ray) */
+    int64_t max_batch_rays;     /* cap on rays gathered into one launch          */
+    int streams;                /* concurrent batch streams (default 3)          */
+    rq_query query;
+    rq_launch launch;
+} rq_server_params;
+
+typedef struct rq_request_stats {
+    double submit_ms;     /* host monotonic clock, ms                           */
+    double start_ms;      /* when its batch was launched                        */
+    double done_ms;       /* when its hits were back in the caller's buffer     */
+    int64_t rays;
+    int32_t batch_id;
+    int32_t status;       /* rq_status of the request                           */
+} rq_request_stats;
+
+rq_status rq_server_create(const rq_server_params* params, rq_server_t* out);
+rq_status rq_server_add_scene(rq_server_t server, rq_scene_t scene, int32_t* scene_id);
+/* host_rays must stay valid and host_hits writable until the request completes.
+ * Pinned host memory gives overlapped copies; pageable memory works too. */
+rq_status rq_server_submit(rq_server_t server, int32_t scene_id, const rq_ray* host_rays,
+                           rq_hit* host_hits, int64_t count, uint64_t* ticket);
+/* timeout_ms < 0 waits without limit. */
+rq_status rq_server_wait(rq_server_t server, uint64_t ticket, int64_t timeout_ms,
+                         rq_request_stats* stats);
+rq_status rq_server_cancel(rq_server_t server, uint64_t ticket);
+rq_status rq_server_destroy(rq_server_t server);
+
+/* ------------------------------------------------- procedural test scenes */
+/*
+ * Seeded synthetic meshes standing in for the reference's missing mesh.dat.
+ * The library allocates *vertices (3*nv floats) and *indices (3*nt ints);
+ * release them with rq_free_mesh.
+ *   heightfield_boxes: (grid+1)^2-vertex heightfield over [0,1]^2, heights
+ *     U[0,1], plus n_boxes axis-aligned boxes (12 triangles each), centres
+ *     U over [0,1]^3, edges U[box_min, box_max].
+ *   city: n_buildings boxes/prisms on a grid with log-normal heights over a
+ *     ground plane.
+ *   spheres_terrain: displaced subdivided spheres over displaced terrain tiles.
+ */
+rq_status rq_gen_heightfield_boxes(uint64_t seed, int grid, int n_boxes, float box_min,
+                                   float box_max, float** vertices, int64_t* nv,
+                                   int32_t** indices, int64_t* nt);
+rq_status rq_gen_city(uint64_t seed, int n_buildings, float** vertices, int64_t* nv,
+                      int32_t** indices, int64_t* nt);
+rq_status rq_gen_spheres_terrain(uint64_t seed, int64_t target_tris, float** vertices,
+                                 int64_t* nv, int32_t** indices, int64_t* nt);
+void rq_free_mesh(float* vertices, int32_t* indices);
+
+/* ----------------------------------------------- reference-shaped adapters */
+/*
+ * Same names, argument meaning and byte layouts as the reference's host entry
+ * points, so a caller written against them links unchanged (float4/Ray/Hit
+ * are passed as void* here; librq also exports C++-linkage overloads with the
+ * exact reference signatures).  One global bound scene per BVH kind, as in the
+ * reference; tracing is synchronous on the legacy default stream and returns
+ * the kernel's error status instead of aborting.
+ *   rtBindCWBVHData  src/TraversalKernelCWBVH.h:3-6 (src/TraversalKernelCWBVH.cu:377-385)
+ *   rtTraceCWBVH     src/TraversalKernelCWBVH.h:8-11 (src/TraversalKernelCWBVH.cu:387-426)
+ *   rtBindBVH2Data   src/TraversalKernelBVH2.h:3-6 (src/TraversalKernelBVH2.cu:180-188)
+ *   rtTraceBVH2      src/TraversalKernelBVH2.h:8-11 (src/TraversalKernelBVH2.cu:190-227)
+ *   GenerateAORaysUniform src/ValidationKernels.h:3-9 (src/ValidationKernels.cu:140-187):
+ *     host surfel arrays in, a new device Ray buffer out (caller frees it with
+ *     cudaFree), tmin 0.01, tmax 1e20, origin offset radius/2.
+ */
+rq_status rq_rtBindCWBVHData(const void* nodes, const void* woop, const int32_t* prim_index);
+rq_status rq_rtTraceCWBVH(void* rays, void* hits, int ray_count);
+rq_status rq_rtBindBVH2Data(const void* nodes, const void* woop, const int32_t* prim_index);
+rq_status rq_rtTraceBVH2(void* rays, void* hits, int ray_count);
+void* rq_GenerateAORaysUniform(int num_texels, int rays_per_texel, const float* pos,
+                               const float* nrm, const float* radius);
+/* Any-hit twins of rtTrace* (the reference has only closest-hit). */
+rq_status rq_rtOccludedCWBVH(void* rays, void* hits, int ray_count);
+rq_status rq_rtOccludedBVH2(void* rays, void* hits, int ray_count);
+
+/* Synchronous device-to-device copy, and cudaFree of a buffer this library
+ * returned (rq_GenerateAORaysUniform). */
+rq_status rq_device_copy(void* dst, const void* src, int64_t bytes);
+rq_status rq_device_free(void* p);
+
+/* ------------------------------------------------------------- device info */
+int rq_device_sm_count(void);
+/* Library build identification: "rq <version> sm_100a". */
+const char* rq_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RQ_H */
