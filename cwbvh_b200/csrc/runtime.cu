@@ -229,8 +229,14 @@ rq_status rq_scene_create(rq_bvh_kind kind, const void* nodes, int64_t node_floa
     if (copy_from_host) {
         sc->owned = true;
         void *dn = nullptr, *dw = nullptr, *dp = nullptr;
-        cudaError_t e = cudaMalloc(&dn, (size_t)node_float4s * 16);
-        if (e == cudaSuccess) e = cudaMalloc(&dw, (size_t)std::max<int64_t>(1, woop_float4s) * 16);
+        // 256 B of zero padding after each buffer: a kernel that loads the
+        // float4s after a BVH2 leaf terminator (as the reference's does,
+        // src/TraversalKernelBVH2.cu:128-133) stays inside the allocation.
+        constexpr size_t kPad = 256;
+        cudaError_t e = cudaMalloc(&dn, (size_t)node_float4s * 16 + kPad);
+        if (e == cudaSuccess) e = cudaMalloc(&dw, (size_t)std::max<int64_t>(1, woop_float4s) * 16 + kPad);
+        if (e == cudaSuccess) e = cudaMemset(dn, 0, (size_t)node_float4s * 16 + kPad);
+        if (e == cudaSuccess) e = cudaMemset(dw, 0, (size_t)std::max<int64_t>(1, woop_float4s) * 16 + kPad);
         if (e == cudaSuccess && sc->prim_count > 0) e = cudaMalloc(&dp, (size_t)sc->prim_count * 4);
         if (e == cudaSuccess) e = cudaMemcpy(dn, nodes, (size_t)node_float4s * 16, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && woop_float4s > 0) e = cudaMemcpy(dw, woop, (size_t)woop_float4s * 16, cudaMemcpyHostToDevice);
