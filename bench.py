@@ -286,10 +286,13 @@ def main():
     ms_sort = time_steps(lambda: rq.lib.rq_batch_run_stage(batch._h, 1, stream.cuda_stream), 3, 1, stream, dist)
     launches_per_step = int(rq.lib.rq_batch_kernel_count(batch._h))
 
-    # ---- clocks during a timed batched region
+    # ---- clocks during a timed batched region (long enough for >= 10 samples)
+    reps = max(args.steps, int(math.ceil(2000.0 / max(ms_batch, 1e-3))))
     clk = Clocks(torch.cuda.current_device())
-    ms_batch2 = time_steps(lambda: batch.run(stream), args.steps, 1, stream, dist)
+    time.sleep(0.3)
+    ms_batch2 = time_steps(lambda: batch.run(stream), reps, 1, stream, dist)
     clocks = clk.stop()
+    clocks["timed_steps"] = reps
 
     # ---- end to end through the public API with host buffers
     host_rays = [torch.empty(r.shape, dtype=r.dtype, pin_memory=True) for r in rays]

@@ -107,14 +107,28 @@ class HostBVH:
     """A converted BVH in host memory (node / Woop / primitive-index buffers)."""
 
     def __init__(self, vertices, indices, kind: int = CWBVH, max_leaf_size: int = 0, sah_bins: int = 0,
-                 max_depth: int = 0, threads: int = 0):
+                 max_depth: int = 0, threads: int = 0, tree: Optional[dict] = None):
+        """Build with the library's SAH builder, or -- with `tree` (the dict
+        shape of HostBVH.tree()) -- convert a tree built elsewhere."""
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         i = np.ascontiguousarray(indices, dtype=np.int32).reshape(-1, 3)
         self.vertices, self.indices, self.kind = v, i, kind
-        bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads)
         h = C.c_void_p()
-        check(lib.rq_build_bvh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0], kind, C.byref(bp),
-                               C.byref(h)), "rq_build_bvh")
+        if tree is None:
+            bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads)
+            check(lib.rq_build_bvh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0], kind, C.byref(bp),
+                                   C.byref(h)), "rq_build_bvh")
+        else:
+            codes = np.ascontiguousarray(tree["codes"], np.int32)
+            boxes = np.ascontiguousarray(tree["boxes"], np.float32)
+            lf = np.ascontiguousarray(tree["leaf_first"], np.int32)
+            lc = np.ascontiguousarray(tree["leaf_count"], np.int32)
+            refs = np.ascontiguousarray(tree["prim_refs"], np.int32)
+            self.kind = kind = CWBVH if tree["width"] == 8 else BVH2
+            check(lib.rq_convert_tree(tree["width"], codes.shape[0], codes.ctypes.data, boxes.ctypes.data,
+                                      lf.size, lf.ctypes.data, lc.ctypes.data, refs.size, refs.ctypes.data,
+                                      int(tree["root_is_leaf"]), v.ctypes.data, v.shape[0], i.ctypes.data,
+                                      i.shape[0], C.byref(h)), "rq_convert_tree")
         self._h = h
         info = N.BVHInfo()
         check(lib.rq_host_bvh_info(h, C.byref(info)), "rq_host_bvh_info")

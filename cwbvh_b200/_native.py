@@ -134,3 +134,6 @@ _sig("rq_device_free", C.c_int, vp)
 def check(status: int, where: str) -> None:
     if status != RQ_OK:
         raise RQError(status, where)
+
+
+_sig("rq_convert_tree", C.c_int, i32, i64, vp, vp, i64, vp, vp, i64, vp, i32, vp, i64, vp, i64, P(vp))

@@ -139,6 +139,108 @@ rq_status rq_host_bvh_tree(rq_host_bvh_t bvh, int32_t* width, int64_t* n_nodes, 
     return RQ_OK;
 }
 
+}  // extern "C"
+
+template <int W>
+static bool import_tree(int64_t n_nodes, const int32_t* codes, const float* boxes, int64_t n_leaves,
+                        const int32_t* lf, const int32_t* lc, int64_t n_refs, const int32_t* refs, bool root_is_leaf,
+                        int64_t nt, Tree<W>& t) {
+    t = Tree<W>();
+    t.root_is_leaf = root_is_leaf;
+    t.prim_refs.assign(refs, refs + n_refs);
+    for (int64_t l = 0; l < n_leaves; ++l) {
+        if (lf[l] < 0 || lc[l] < 0 || (int64_t)lf[l] + lc[l] > n_refs) return false;
+        if (W == 8 && (lc[l] < 1 || lc[l] > 3)) return false;
+        t.leaves.push_back(Leaf{lf[l], lc[l]});
+    }
+    for (int32_t r : t.prim_refs)
+        if (r < 0 || r >= nt) return false;
+    for (int64_t n = 0; n < n_nodes; ++n) {
+        TreeNode<W> nd{};
+        int count = 0;
+        for (int c = 0; c < W; ++c) {
+            const int32_t code = codes[n * W + c];
+            if (code >= n_nodes || (code <= -2 && -code - 2 >= n_leaves)) return false;
+            if (code != -1 && c != count) return false;  // children occupy slots 0..count-1
+            nd.child[c] = code;
+            if (code != -1) ++count;
+            for (int a = 0; a < 3; ++a) {
+                nd.lo[c][a] = boxes[(n * W + c) * 6 + a];
+                nd.hi[c][a] = boxes[(n * W + c) * 6 + 3 + a];
+            }
+        }
+        nd.count = count;
+        t.nodes.push_back(nd);
+    }
+    if (root_is_leaf && n_leaves < 1) return false;
+    if (!root_is_leaf && n_nodes < 1) return false;
+    // A tree: the root is nobody's child and every other node has one parent,
+    // so the converters' depth-first walks end.
+    std::vector<uint8_t> parents(t.nodes.size(), 0);
+    for (const auto& nd : t.nodes)
+        for (int c = 0; c < W; ++c)
+            if (nd.child[c] >= 0 && ++parents[nd.child[c]] > 1) return false;
+    if (!t.nodes.empty() && parents[0] != 0) return false;
+    Box b;
+    for (const auto& nd : t.nodes)
+        for (int c = 0; c < nd.count; ++c) {
+            b.grow(v3(nd.lo[c][0], nd.lo[c][1], nd.lo[c][2]));
+            b.grow(v3(nd.hi[c][0], nd.hi[c][1], nd.hi[c][2]));
+        }
+    t.bounds = b;
+    return true;
+}
+
+extern "C" {
+
+rq_status rq_convert_tree(int32_t width, int64_t n_nodes, const int32_t* child_codes, const float* child_boxes,
+                          int64_t n_leaves, const int32_t* leaf_first, const int32_t* leaf_count, int64_t n_prim_refs,
+                          const int32_t* prim_refs, int32_t root_is_leaf, const float* vertices, int64_t nv,
+                          const int32_t* indices, int64_t nt, rq_host_bvh_t* out) {
+    if (!out || (width != 2 && width != 8) || n_nodes < 0 || n_leaves < 0 || n_prim_refs < 0 || nv < 0 || nt < 0)
+        return RQ_ERR_INVALID_ARG;
+    if ((n_nodes > 0 && (!child_codes || !child_boxes)) || (n_leaves > 0 && (!leaf_first || !leaf_count)) ||
+        (n_prim_refs > 0 && !prim_refs) || (nt > 0 && (!indices || !vertices)))
+        return RQ_ERR_INVALID_ARG;
+    if (width == 8 && root_is_leaf) return RQ_ERR_INVALID_ARG;  // the CWBVH root is an inner node
+    for (int64_t k = 0; k < 3 * nt; ++k)
+        if (indices[k] < 0 || indices[k] >= nv) return RQ_ERR_INVALID_ARG;
+    rq_host_bvh* h = new (std::nothrow) rq_host_bvh();
+    if (!h) return RQ_ERR_OOM;
+    try {
+        Mesh m;
+        m.v.assign(vertices, vertices + 3 * nv);
+        m.i.assign(indices, indices + 3 * nt);
+        bool ok;
+        if (width == 2) {
+            h->b.kind = RQ_BVH_BVH2;
+            ok = import_tree<2>(n_nodes, child_codes, child_boxes, n_leaves, leaf_first, leaf_count, n_prim_refs,
+                                prim_refs, root_is_leaf != 0, nt, h->b.tree2);
+            if (ok) {
+                convert_bvh2(h->b.tree2, m, h->b);
+                h->b.depth = tree_depth2(h->b.tree2);
+            }
+        } else {
+            h->b.kind = RQ_BVH_CWBVH;
+            ok = import_tree<8>(n_nodes, child_codes, child_boxes, n_leaves, leaf_first, leaf_count, n_prim_refs,
+                                prim_refs, false, nt, h->b.tree8);
+            if (ok) {
+                convert_cwbvh(h->b.tree8, m, h->b);
+                h->b.depth = tree_depth8(h->b.tree8);
+            }
+        }
+        if (!ok) {
+            delete h;
+            return RQ_ERR_INVALID_ARG;
+        }
+    } catch (const std::bad_alloc&) {
+        delete h;
+        return RQ_ERR_OOM;
+    }
+    *out = h;
+    return RQ_OK;
+}
+
 rq_status rq_woopify(const float v0[3], const float v1[3], const float v2[3], float out_rows[12]) {
     if (!v0 || !v1 || !v2 || !out_rows) return RQ_ERR_INVALID_ARG;
     woopify(v3(v0[0], v0[1], v0[2]), v3(v1[0], v1[1], v1[2]), v3(v2[0], v2[1], v2[2]), out_rows);

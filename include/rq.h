@@ -120,6 +120,17 @@ rq_status rq_host_bvh_tree(rq_host_bvh_t bvh, int32_t* width, int64_t* n_nodes, 
                            float* child_boxes, int32_t* leaf_first, int32_t* leaf_count,
                            int32_t* prim_refs);
 
+/* Convert a caller-built tree (same arrays as rq_host_bvh_tree; width 2 ->
+ * BVH2 layout, 8 -> CWBVH layout) over the given mesh.  The counterpart of
+ * ConvertToGPUBVH2 / ConvertToGPUCompressedWideBVH (src/GPUBVHConverter.h:
+ * 13-26), which take a BVHNNode tree from an external builder.  CWBVH leaves
+ * must hold 1..3 triangles and nodes at most 8 children in slots 0..n-1. */
+rq_status rq_convert_tree(int32_t width, int64_t n_nodes, const int32_t* child_codes,
+                          const float* child_boxes, int64_t n_leaves, const int32_t* leaf_first,
+                          const int32_t* leaf_count, int64_t n_prim_refs, const int32_t* prim_refs,
+                          int32_t root_is_leaf, const float* vertices, int64_t nv,
+                          const int32_t* indices, int64_t nt, rq_host_bvh_t* out);
+
 /* Woop transform of one triangle: 3 float4 rows (V0, V1, V2) as
  * WoopifyTriangle emits them (src/GPUBVHConverter.cpp:380-403). */
 rq_status rq_woopify(const float v0[3], const float v1[3], const float v2[3], float out_rows[12]);

@@ -1,0 +1,182 @@
+"""Converter parity with the reference's ConvertToGPUBVH2 /
+ConvertToGPUCompressedWideBVH / WoopifyTriangle (src/GPUBVHConverter.cpp),
+pinned by tests/golden/convert_fixtures.npz (made by the reference's own code,
+tests/golden/make_golden.py)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+FIX = Path(__file__).resolve().parent / "golden" / "convert_fixtures.npz"
+SCENES = ["hfbox", "flat", "quads", "one_tri", "city"]
+
+
+@pytest.fixture(scope="module")
+def fx():
+    return np.load(FIX)
+
+
+def _tree(fx, name, tag):
+    p = f"{name}/{tag}/tree/"
+    return {"width": 8 if tag == "cw" else 2, "codes": fx[p + "codes"], "boxes": fx[p + "boxes"],
+            "leaf_first": fx[p + "leaf_first"], "leaf_count": fx[p + "leaf_count"],
+            "prim_refs": fx[p + "prim_refs"], "root_is_leaf": bool(fx[p + "root_is_leaf"])}
+
+
+def _woop_close(a, b):
+    """Woop rows agree to float rounding of the matrix inverse: the reference
+    inverts in float, this library in double."""
+    scale = np.maximum(np.abs(b).max(axis=1, keepdims=True), 1e-6)
+    return np.abs(a - b) <= 2e-4 * scale
+
+
+@pytest.mark.parametrize("name", SCENES)
+@pytest.mark.parametrize("tag", ["cw", "b2"])
+def test_nodes_byte_identical(rq, fx, name, tag):
+    V, I = fx[f"{name}/V"], fx[f"{name}/I"]
+    hb = rq.HostBVH(V, I, tree=_tree(fx, name, tag))
+    ref_nodes = fx[f"{name}/{tag}/ref/nodes"]
+    assert hb.nodes.shape == ref_nodes.shape
+    assert np.array_equal(hb.nodes.view(np.uint32), ref_nodes.view(np.uint32))
+    assert np.array_equal(hb.prim_index, fx[f"{name}/{tag}/ref/prim"])
+
+
+@pytest.mark.parametrize("name", SCENES)
+@pytest.mark.parametrize("tag", ["cw", "b2"])
+def test_woop_rows(rq, fx, name, tag):
+    V, I = fx[f"{name}/V"], fx[f"{name}/I"]
+    hb = rq.HostBVH(V, I, tree=_tree(fx, name, tag))
+    ref = fx[f"{name}/{tag}/ref/woop"]
+    assert hb.woop.shape == ref.shape
+    # Walk the primitive map: a triangle is [prim, -1, -1] (its V0 row
+    # first), a BVH2 leaf terminator is a lone -1.
+    prim = hb.prim_index
+    v0 = np.zeros(prim.size, bool)
+    term = np.zeros(prim.size, bool)
+    i = 0
+    while i < prim.size:
+        if prim[i] >= 0:
+            v0[i] = True
+            i += 3
+        else:
+            term[i] = True
+            i += 1
+    bits = hb.woop.view(np.uint32)[:, 0]
+    ref_bits = ref.view(np.uint32)[:, 0]
+    assert (bits[term] == 0x80000000).all() and (ref_bits[term] == 0x80000000).all()
+    # V0.x is never the terminator pattern here (the reference's float
+    # inverse can produce -0.0f there, src/TraversalKernelBVH2.cu:132).
+    assert not (bits[v0] == 0x80000000).any()
+    rows = ~term
+    # Compare triangle by triangle (3 rows each).
+    a = hb.woop[rows].reshape(-1, 12)
+    b = ref[rows].reshape(-1, 12)
+    assert _woop_close(a, b).all()
+
+
+def test_woopify_against_reference(rq, fx):
+    tris, ref_rows = fx["woopify/tris"], fx["woopify/ref_rows"]
+    for k, t in enumerate(tris):
+        mine = rq.woopify(t[0], t[1], t[2])
+        if k == 0:
+            # Degenerate (collinear): zero rows that no ray can hit; the
+            # reference substitutes the identity (a unit triangle at z = 0).
+            assert not mine.any()
+            assert np.array_equal(ref_rows[k], np.array([[0, 0, 1, -0.0], [1, 0, 0, 0], [0, 1, 0, 0]], np.float32))
+            continue
+        assert _woop_close(mine.reshape(1, 12), ref_rows[k].reshape(1, 12)).all(), k
+        assert mine.view(np.uint32)[0, 0] != 0x80000000  # never a BVH2 leaf terminator
+
+
+def _decode_cwbvh(nodes):
+    """Boxes of every child slot of every CWBVH node: p + q * 2^e."""
+    n = nodes.reshape(-1, 5, 4)
+    out = []
+    for nd in n:
+        p = nd[0, :3].astype(np.float64)
+        e = nd[0, 3:4].view(np.uint8)[:3].view(np.int8).astype(np.int64)
+        q = nd[2:5].reshape(-1).view(np.uint8).reshape(6, 8)  # qlo.x qlo.y qlo.z qhi.x qhi.y qhi.z
+        meta = nd[1, 2:4].view(np.uint8)
+        scale = np.ldexp(1.0, e)
+        lo = p[:, None] + q[0:3] * scale[:, None]
+        hi = p[:, None] + q[3:6] * scale[:, None]
+        out.append((lo, hi, meta))
+    return out
+
+
+@pytest.mark.parametrize("name", SCENES)
+def test_cwbvh_boxes_conservative(rq, fx, name):
+    """Every quantised child box contains the child's exact box."""
+    V, I = fx[f"{name}/V"], fx[f"{name}/I"]
+    tr = _tree(fx, name, "cw")
+    hb = rq.HostBVH(V, I, tree=tr)
+    # Walk the converted nodes in the converter's order, pairing slots with
+    # the tree's boxes through the same greedy slot assignment is not
+    # needed: a child's box must be contained in exactly one decoded slot.
+    dec = _decode_cwbvh(hb.nodes)
+    boxes = tr["boxes"].reshape(-1, 6)
+    boxes = boxes[np.isfinite(boxes).all(axis=1) & (tr["codes"].reshape(-1) != -1)]
+    all_lo = np.concatenate([d[0].T[d[2] != 0] for d in dec])
+    all_hi = np.concatenate([d[1].T[d[2] != 0] for d in dec])
+    for b in boxes:
+        inside = (all_lo <= b[:3] + 0).all(axis=1) & (all_hi >= b[3:] - 0).all(axis=1)
+        assert inside.any()
+
+
+def test_quantisation_overflow_guard(rq, po):
+    """A node whose extent / 255 lies just above a power of two: log2f rounds
+    down, and the reference's upper bound rounds up to 256, which its uint8
+    store wraps to 0 (src/GPUBVHConverter.cpp:306-316).  The converter here
+    takes the next exponent, so the child box stays conservative."""
+    ext = np.float32(255.0 * 2.0 ** -7 * (1 + 2.0 ** -22))
+    V = np.array([[0, 0, 0], [0.5, 0.1, 0.1], [0.2, 0.3, 0.2],
+                  [0.5, 0, 0], [ext, 0.1, 0.1], [0.7, 0.3, 0.2]], np.float32)
+    I = np.array([[0, 1, 2], [3, 4, 5]], np.int32)
+    codes = np.full((1, 8), -1, np.int32)
+    codes[0, 0], codes[0, 1] = -2, -3
+    boxes = np.zeros((1, 8, 6), np.float32)
+    boxes[0, 0] = [0, 0, 0, 0.5, 0.3, 0.2]
+    boxes[0, 1] = [0.5, 0, 0, ext, 0.3, 0.2]
+    tree = {"width": 8, "codes": codes, "boxes": boxes, "leaf_first": np.array([0, 1], np.int32),
+            "leaf_count": np.array([1, 1], np.int32), "prim_refs": np.array([0, 1], np.int32), "root_is_leaf": False}
+    hb = rq.HostBVH(V, I, tree=tree)
+    (lo, hi, meta), = _decode_cwbvh(hb.nodes)
+    for s in np.nonzero(meta)[0]:
+        assert hi[0, s] >= lo[0, s]
+    assert hi[0][meta != 0].max() >= ext
+    if po.ref_available():
+        nodes, _, _ = po.ref_convert(tree, V, I)
+        (rlo, rhi, rmeta), = _decode_cwbvh(nodes)
+        assert (rhi[0][rmeta != 0] < ext).any()  # the reference's wrapped bound
+
+
+def test_convert_tree_rejects_bad_trees(rq):
+    V = np.zeros((3, 3), np.float32)
+    I = np.array([[0, 1, 2]], np.int32)
+    codes = np.array([[0, -2, -1, -1, -1, -1, -1, -1]], np.int32)  # the root as its own child
+    boxes = np.zeros((1, 8, 6), np.float32)
+    bad = {"width": 8, "codes": codes, "boxes": boxes, "leaf_first": np.array([0], np.int32),
+           "leaf_count": np.array([1], np.int32), "prim_refs": np.array([0], np.int32), "root_is_leaf": False}
+    with pytest.raises(rq.RQError):
+        rq.HostBVH(V, I, tree=bad)
+    bad["codes"] = np.array([[-1, -2, -1, -1, -1, -1, -1, -1]], np.int32)  # a gap before a child
+    with pytest.raises(rq.RQError):
+        rq.HostBVH(V, I, tree=bad)
+    bad["codes"] = np.array([[-2, -1, -1, -1, -1, -1, -1, -1]], np.int32)
+    bad["leaf_count"] = np.array([4], np.int32)  # CWBVH leaves hold at most 3 triangles
+    with pytest.raises(rq.RQError):
+        rq.HostBVH(V, I, tree=bad)
+
+
+def test_builder_invariants(rq):
+    """Leaves hold <= 3 triangles (CWBVH), every triangle is referenced once,
+    and the depth stays within the traversal stacks."""
+    from cwbvh_b200 import workloads as W
+    V, I = W.scene_of_size(4, 50_000)
+    hb = rq.HostBVH(V, I, rq.CWBVH)
+    tr = hb.tree()
+    assert tr["leaf_count"].max() <= 3 and tr["leaf_count"].min() >= 1
+    assert np.array_equal(np.sort(tr["prim_refs"]), np.arange(I.shape[0]))
+    assert 2 * hb.info["depth"] <= 64
+    hb2 = rq.HostBVH(V, I, rq.BVH2)
+    assert hb2.info["depth"] <= 31
