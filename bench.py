@@ -213,6 +213,7 @@ def main():
     ap.add_argument("--workload", default="batched", choices=["batched", "small"])
     ap.add_argument("--quick", action="store_true", help="8 smaller scenes (smoke runs)")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -331,7 +332,7 @@ def main():
 
     # ---- CPU baseline (oracle restatement, all host threads, bounded sample)
     cpu = None
-    if rank == 0 and world >= 1:
+    if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(spec, built)
 
     world_rays = total_rays * world
