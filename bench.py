@@ -313,12 +313,13 @@ def main():
 
     # ---- algorithmic bytes per ray: 32 (ray) + 16 (hit) + 80 per node + 48 per triangle
     nodes_total, tris_total = 0, 0
-    for ds, r in zip(scenes, rays):
-        hh = torch.empty((r.shape[0], 4), device="cuda")
-        nv, nt = rq.trace_counted(ctx, ds.scene, r, hh, rq.ANY, stream=stream)
-        nodes_total += int(nv.sum().item())
-        tris_total += int(nt.sum().item())
-        del hh, nv, nt
+    with torch.cuda.stream(stream):  # counters are allocated, written and summed on one stream
+        for ds, r in zip(scenes, rays):
+            hh = torch.empty((r.shape[0], 4), device="cuda")
+            nv, nt = rq.trace_counted(ctx, ds.scene, r, hh, rq.ANY, stream=stream)
+            nodes_total += int(nv.sum(dtype=torch.int64).item())
+            tris_total += int(nt.sum(dtype=torch.int64).item())
+            del hh, nv, nt
     ctx.check(stream)
     alg_bytes = 48 * total_rays + 80 * nodes_total + 48 * tris_total
     peak, peak_kind = measured_peak_hbm()

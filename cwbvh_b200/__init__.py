@@ -55,6 +55,24 @@ def _stream(stream) -> int:
     return stream.cuda_stream
 
 
+class _On:
+    """Allocate on the stream the work goes to (no-op for the current stream)."""
+
+    def __init__(self, stream):
+        self.stream = stream
+        self.ctx = None
+
+    def __enter__(self):
+        if self.stream is not None and not isinstance(self.stream, int):
+            import torch
+            self.ctx = torch.cuda.stream(self.stream)
+            self.ctx.__enter__()
+
+    def __exit__(self, *exc):
+        if self.ctx is not None:
+            self.ctx.__exit__(*exc)
+
+
 def _rows(t, width: int, what: str) -> int:
     n = t.numel() * t.element_size()
     if n % (width * 4):
@@ -267,8 +285,9 @@ def trace_counted(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stre
     """Trace and return per-ray (node fetches, triangle tests) as int32 tensors."""
     import torch
     n = _rows(rays, 8, "rays")
-    nv = torch.zeros(n, dtype=torch.int32, device=rays.device)
-    nt = torch.zeros(n, dtype=torch.int32, device=rays.device)
+    with _On(stream):
+        nv = torch.zeros(n, dtype=torch.int32, device=rays.device)
+        nt = torch.zeros(n, dtype=torch.int32, device=rays.device)
     check(lib.rq_trace_counted(ctx._h, scene._h, _ptr(rays), _ptr(hits), n, query, _ptr(nv), _ptr(nt),
                                _stream(stream)), "rq_trace_counted")
     return nv, nt
@@ -280,7 +299,8 @@ def aorays(pos, nrm, radius, spp: int, seed: int = 0, tmin: float = 0.01, tmax: 
     import torch
     ns = _rows(pos, 4, "pos")
     if out is None:
-        out = torch.empty((ns * spp, 8), dtype=torch.float32, device=pos.device)
+        with _On(stream):
+            out = torch.empty((ns * spp, 8), dtype=torch.float32, device=pos.device)
     check(lib.rq_aorays(_ptr(pos), _ptr(nrm), _ptr(radius) or None, ns, spp, seed, tmin, tmax, offset_scale,
                         _ptr(out), _stream(stream)), "rq_aorays")
     return out
@@ -290,9 +310,10 @@ def sample_surfels(vertices, indices, n: int, seed: int = 0, stream=None):
     """n surfels at uniform (triangle, barycentric) points of a device mesh."""
     import torch
     dev = vertices.device
-    pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
-    nrm = torch.empty((n, 4), dtype=torch.float32, device=dev)
-    rad = torch.empty((n,), dtype=torch.float32, device=dev)
+    with _On(stream):
+        pos = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        nrm = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        rad = torch.empty((n,), dtype=torch.float32, device=dev)
     nt = indices.numel() // 3
     check(lib.rq_sample_surfels(_ptr(vertices), _ptr(indices), nt, n, seed, _ptr(pos), _ptr(nrm), _ptr(rad),
                                 _stream(stream)), "rq_sample_surfels")
@@ -301,7 +322,8 @@ def sample_surfels(vertices, indices, n: int, seed: int = 0, stream=None):
 
 def ao_reduce(hits, n_surfels: int, spp: int, stream=None):
     import torch
-    ao = torch.empty(n_surfels, dtype=torch.float32, device=hits.device)
+    with _On(stream):
+        ao = torch.empty(n_surfels, dtype=torch.float32, device=hits.device)
     check(lib.rq_ao_reduce(_ptr(hits), n_surfels, spp, _ptr(ao), _stream(stream)), "rq_ao_reduce")
     return ao
 
@@ -309,8 +331,9 @@ def ao_reduce(hits, n_surfels: int, spp: int, stream=None):
 def sort_rays(ctx: Context, rays, bounds_lo, bounds_hi, stream=None):
     import torch
     n = _rows(rays, 8, "rays")
-    out = torch.empty_like(rays)
-    perm = torch.empty(n, dtype=torch.int32, device=rays.device)
+    with _On(stream):
+        out = torch.empty_like(rays)
+        perm = torch.empty(n, dtype=torch.int32, device=rays.device)
     lo = (C.c_float * 3)(*bounds_lo)
     hi = (C.c_float * 3)(*bounds_hi)
     check(lib.rq_sort_rays(ctx._h, _ptr(rays), n, lo, hi, _ptr(out), _ptr(perm), _stream(stream)), "rq_sort_rays")

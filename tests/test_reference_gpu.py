@@ -1,0 +1,94 @@
+"""The reference's own CUDA kernels (oracle/_ref, compiled unmodified from the
+reference sources for sm_100a) on the same buffers and rays: the oracle and
+this library agree with them up to FP64-adjudicated ties (the reference uses
+an approximate 1/x under -use_fast_math).  Also the drop-in adapters with the
+reference's entry-point names."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from adjudicate import compare, prim_ids
+
+pytestmark = pytest.mark.gpu
+
+
+def _buffers(rq, scene):
+    n, w, p = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    rq.check(rq.lib.rq_scene_device_buffers(scene._h, C.byref(n), C.byref(w), C.byref(p)), "buffers")
+    return n, w, p
+
+
+@pytest.fixture(scope="module")
+def setup(rq):
+    import torch
+    from cwbvh_b200 import workloads as W
+    V, I = W.heightfield_boxes(0)
+    scenes = {k: W.upload(V, I, k) for k in (rq.CWBVH, rq.BVH2)}
+    rays = W.ao_rays(scenes[rq.CWBVH], 100_000, seed=1000)
+    torch.cuda.synchronize()
+    return V, I, scenes, rays
+
+
+@pytest.mark.parametrize("kind", [0, 1], ids=["cwbvh", "bvh2"])
+def test_reference_kernel_vs_oracle_and_rq(rq, po, setup, kind):
+    import torch
+    if not po.ref_available():
+        pytest.skip("oracle/_ref not built")
+    V, I, scenes, rays = setup
+    ds = scenes[kind]
+    # The reference kernels have fixed stacks without overflow checks: 40
+    # entries (CWBVH, 2 per level) and 32 (BVH2, 1 per level + sentinel).
+    depth = ds.host.info["depth"]
+    assert (2 * depth <= 40) if kind == rq.CWBVH else (depth <= 31)
+    lib = po.ref()
+    n, w, p = _buffers(rq, ds.scene)
+    hits = torch.full((rays.shape[0], 4), float("nan"), device="cuda")
+    if kind == rq.CWBVH:
+        lib.ref_bind_cwbvh(n, w, p)
+        lib.ref_trace_cwbvh(rays.data_ptr(), hits.data_ptr(), rays.shape[0])
+    else:
+        lib.ref_bind_bvh2(n, w, p)
+        lib.ref_trace_bvh2(rays.data_ptr(), hits.data_ptr(), rays.shape[0])
+    assert lib.ref_sync() == 0
+    ref = hits.cpu().numpy()
+    written = ~np.isnan(ref[:, 0])
+    r = rays.cpu().numpy()
+    # Coverage: every ray must be written once.  (The reference's persistent
+    # loop can drop a ray whose popped triangle group meets a fetch break;
+    # any such ray is reported, not compared.)
+    lost = int((~written).sum())
+    assert lost <= rays.shape[0] // 1000, lost
+    want = po.trace(kind, ds.host.nodes, ds.host.woop, r[written], False)
+    compare(po, r[written], ref[written], want, ds.host.prim_index, V, I, any_hit=False)
+    mine = torch.empty_like(hits)
+    ctx = rq.Context()
+    rq.trace(ctx, ds.scene, rays, mine, rq.ANY)
+    ctx.check()
+    m = mine.cpu().numpy()
+    compare(po, r[written], m[written], ref[written], ds.host.prim_index, V, I, any_hit=True)
+
+
+@pytest.mark.parametrize("kind", [0, 1], ids=["cwbvh", "bvh2"])
+def test_dropin_adapters(rq, po, setup, kind):
+    """rtBind*/rtTrace* with the reference's argument meaning (device
+    pointers, one bound scene, synchronous) and their any-hit twins."""
+    import torch
+    V, I, scenes, rays = setup
+    ds = scenes[kind]
+    hb = ds.host
+    nodes = torch.from_numpy(hb.nodes).cuda()
+    woop = torch.from_numpy(hb.woop).cuda()
+    prim = torch.from_numpy(hb.prim_index).cuda()
+    bind = rq.rtBindCWBVHData if kind == rq.CWBVH else rq.rtBindBVH2Data
+    trace = rq.rtTraceCWBVH if kind == rq.CWBVH else rq.rtTraceBVH2
+    occl = rq.rtOccludedCWBVH if kind == rq.CWBVH else rq.rtOccludedBVH2
+    bind(nodes, woop, prim)
+    hits = torch.empty((rays.shape[0], 4), device="cuda")
+    trace(rays, hits, rays.shape[0])
+    r = rays.cpu().numpy()
+    want = po.trace(kind, hb.nodes, hb.woop, r, False)
+    compare(po, r, hits.cpu().numpy(), want, hb.prim_index, V, I, any_hit=False)
+    occl(rays, hits, rays.shape[0])
+    wa = po.trace(kind, hb.nodes, hb.woop, r, True)
+    assert np.array_equal(prim_ids(hits.cpu().numpy(), hb.prim_index) >= 0, prim_ids(wa, hb.prim_index) >= 0)

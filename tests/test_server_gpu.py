@@ -1,0 +1,129 @@
+"""Continuous-batching server: every request's result is the same alone and in
+the mix; requests arriving while others run are admitted and overlap; failures
+(unknown scene, over-budget request, cancellation, shutdown) come back as
+status codes."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from adjudicate import prim_ids
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def scenes(rq):
+    import torch
+    from cwbvh_b200 import workloads as W
+    out = []
+    for seed, tris in ((0, 20000), (1, 60000), (2, 5000)):
+        V, I = W.scene_of_size(seed, tris)
+        ds = W.upload(V, I, rq.CWBVH)
+        out.append(ds)
+    torch.cuda.synchronize()
+    return out
+
+
+def _rays(W, ds, n, seed):
+    return W.ao_rays(ds, n, seed=seed).cpu().numpy()
+
+
+def _pinned(shape):
+    import torch
+    return torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+
+
+def test_results_same_alone_and_in_mix(rq, scenes):
+    from cwbvh_b200 import workloads as W
+    rng = np.random.default_rng(0)
+    reqs = []
+    for k in range(24):
+        sid = int(rng.integers(0, len(scenes)))
+        n = int(np.exp(rng.uniform(np.log(4000), np.log(200_000))))
+        rays = _pinned((n, 8))
+        rays[:] = _rays(W, scenes[sid], n, 100 + k)
+        reqs.append((sid, rays))
+    # alone: one request at a time
+    alone = []
+    srv = rq.Server(hbm_budget_bytes=1 << 30, query=rq.ANY, streams=3)
+    ids = [srv.add_scene(ds.scene) for ds in scenes]
+    for sid, rays in reqs:
+        hits = _pinned((rays.shape[0], 4))
+        t = srv.submit(ids[sid], rays, hits)
+        st = srv.wait(t)
+        assert st["status"] == 0
+        alone.append(hits.copy())
+    # in the mix: all submitted at once from two threads, pageable and pinned buffers
+    mix = [None] * len(reqs)
+    tickets = [None] * len(reqs)
+
+    def submitter(ks):
+        for k in ks:
+            sid, rays = reqs[k]
+            hits = np.zeros((rays.shape[0], 4), np.float32) if k % 2 else _pinned((rays.shape[0], 4))
+            mix[k] = hits
+            tickets[k] = srv.submit(ids[sid], rays, hits)
+            time.sleep(0.001)
+
+    th = [threading.Thread(target=submitter, args=(range(j, len(reqs), 2),)) for j in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    stats = [srv.wait(t) for t in tickets]
+    srv.close()
+    batches = {s["batch_id"] for s in stats}
+    assert len(batches) < len(reqs)  # requests were gathered into shared launches
+    for k, (sid, rays) in enumerate(reqs):
+        pi = scenes[sid].host.prim_index
+        assert np.array_equal(prim_ids(alone[k], pi) >= 0, prim_ids(mix[k], pi) >= 0), k
+    lat = np.array([s["done_ms"] - s["submit_ms"] for s in stats])
+    assert np.isfinite(np.percentile(lat, 99))
+
+
+def test_results_match_plain_trace(rq, scenes):
+    import torch
+    from cwbvh_b200 import workloads as W
+    srv = rq.Server(hbm_budget_bytes=256 << 20, query=rq.ANY, streams=2)
+    sid = srv.add_scene(scenes[1].scene)
+    rays = _pinned((100_000, 8))
+    rays[:] = _rays(W, scenes[1], 100_000, 7)
+    hits = _pinned((100_000, 4))
+    srv.wait(srv.submit(sid, rays, hits))
+    srv.close()
+    ctx = rq.Context()
+    h = torch.empty((100_000, 4), device="cuda")
+    rq.trace(ctx, scenes[1].scene, torch.from_numpy(rays).cuda(), h, rq.ANY)
+    ctx.check()
+    pi = scenes[1].host.prim_index
+    assert np.array_equal(prim_ids(hits, pi) >= 0, prim_ids(h.cpu().numpy(), pi) >= 0)
+
+
+def test_failures_are_status_codes(rq, scenes):
+    from cwbvh_b200 import workloads as W
+    srv = rq.Server(hbm_budget_bytes=48 * 3 * 50_000, query=rq.ANY, streams=3)  # 50k rays per worker
+    sid = srv.add_scene(scenes[0].scene)
+    rays = _pinned((60_000, 8))
+    rays[:] = _rays(W, scenes[0], 60_000, 9)
+    hits = _pinned((60_000, 4))
+    with pytest.raises(rq.RQError) as e:
+        srv.submit(sid, rays, hits)  # larger than a worker arena
+    assert e.value.status == 8  # RQ_ERR_BUDGET
+    with pytest.raises(rq.RQError) as e:
+        srv.submit(99, rays[:10], hits[:10])
+    assert e.value.status == 7  # RQ_ERR_NOT_FOUND
+    with pytest.raises(rq.RQError) as e:
+        srv.wait(123456)
+    assert e.value.status == 7
+    # Queue more than the workers can hold; cancel the last queued one.
+    tickets = [srv.submit(sid, rays[:40_000], hits[:40_000]) for _ in range(8)]
+    cancelled = srv.cancel(tickets[-1])
+    for t in tickets[:-1]:
+        assert srv.wait(t)["status"] == 0
+    if cancelled == 0:
+        with pytest.raises(rq.RQError) as e:
+            srv.wait(tickets[-1])
+        assert e.value.status == 9  # RQ_ERR_CANCELLED
+    srv.close()
