@@ -9,7 +9,11 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "librq.so"
+import os
+
+# RQ_LIBRARY points at another build of librq.so (for comparing builds);
+# by default the in-tree library next to this file is loaded.
+LIB_PATH = Path(os.environ.get("RQ_LIBRARY") or (Path(__file__).resolve().parent / "librq.so"))
 
 if not LIB_PATH.exists():
     raise ImportError(f"{LIB_PATH} is missing: build it with `python cwbvh_b200/build.py`")

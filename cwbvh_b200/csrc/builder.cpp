@@ -2,8 +2,8 @@
 // (BuildBVH2Triangle / BuildBVH8Triangle, src/EmbreeBVHBuilder.cpp:303-478),
 // which is not available here.  A binary tree is built top-down with a binned
 // surface-area heuristic (object splits only; no spatial splits), then the
-// 8-wide tree for the CWBVH is made by greedily opening the largest-area inner
-// child until a node has 8 children.  Leaves of the 8-wide tree hold at most 3
+// 8-wide tree for the CWBVH is made by collapsing it with a surface-area
+// cost model (see collapse_optimal).  Leaves of the 8-wide tree hold at most 3
 // triangles, as the reference asks Embree for (maxLeafSize = 3,
 // src/EmbreeBVHBuilder.cpp:456-457).
 //
@@ -272,6 +272,167 @@ void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool 
     out.leaves = std::move(b.leaves);
 }
 
+// Optimal collapse of a binary tree into an 8-wide tree under a surface-area
+// cost model.  For every binary node n and k = 1..8, best[n][k] is the least
+// cost of representing the subtree of n with at most k children ("slots") of
+// an 8-wide node:
+//   k = 1:  one leaf holding all of n's triangles (when there are <= 3), or
+//           an 8-wide node of its own: kNodeCost * area(n) plus n's two
+//           children distributed over 8 slots;
+//   k > 1:  the k = 1 choice, or n opened: best[c0][j] + best[c1][k - j].
+// A leaf costs kLeafCost * area * triangles.  The choices are replayed
+// top-down to emit the nodes.  Compared with greedily opening the largest
+// child this fills the slots (fewer, fuller nodes) and merges small subtrees
+// into leaves of up to 3 triangles.
+namespace {
+constexpr float kNodeCost = 1.0f;
+constexpr float kLeafCost = 0.3f;
+
+struct Collapse {
+    struct Child {
+        int32_t code;  // binary child code
+        const float* lo;
+        const float* hi;
+    };
+
+    const Tree<2>& t;
+    std::vector<float> best;   // [node * 9 + k], k = 1..8
+    std::vector<uint8_t> how;  // [node * 9 + k]: 0 leaf, 1 own node, 2 + j opened with j slots to child 0
+    std::vector<uint8_t> node_split;  // slots to child 0 when the node is an 8-wide node of its own
+    std::vector<int32_t> prims;
+
+    explicit Collapse(const Tree<2>& tree) : t(tree) {}
+
+    static float box_area(const float* lo, const float* hi) {
+        const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+        if (!(dx >= 0.f && dy >= 0.f && dz >= 0.f)) return 0.f;
+        return 2.f * (dx * dy + dy * dz + dz * dx);
+    }
+    int32_t count_of(int32_t code) const { return code >= 0 ? prims[code] : t.leaves[-code - 2].count; }
+    float cost(int32_t code, int k, float a) const {
+        if (code >= 0) return best[(size_t)code * 9 + k];
+        return kLeafCost * a * (float)t.leaves[-code - 2].count;  // a binary leaf stays one leaf
+    }
+
+    void run() {
+        const size_t n = t.nodes.size();
+        best.assign(n * 9, INFINITY);
+        how.assign(n * 9, 0);
+        node_split.assign(n, 4);
+        prims.assign(n, 0);
+        // Post-order (parallel builds interleave node numbering).
+        std::vector<int32_t> order;
+        order.reserve(n);
+        std::vector<std::pair<int32_t, bool>> st{{0, false}};
+        while (!st.empty()) {
+            auto [v, done] = st.back();
+            st.pop_back();
+            if (done) {
+                order.push_back(v);
+                continue;
+            }
+            st.push_back({v, true});
+            for (int c = 0; c < 2; ++c)
+                if (t.nodes[v].child[c] >= 0) st.push_back({t.nodes[v].child[c], false});
+        }
+        for (int32_t v : order) {
+            const TreeNode<2>& nd = t.nodes[v];
+            const float ca[2] = {box_area(nd.lo[0], nd.hi[0]), box_area(nd.lo[1], nd.hi[1])};
+            BBox b;
+            b.grow(nd.lo[0], nd.hi[0]);
+            b.grow(nd.lo[1], nd.hi[1]);
+            const float av = b.area();
+            prims[v] = count_of(nd.child[0]) + count_of(nd.child[1]);
+            float open[9];
+            uint8_t split[9];
+            for (int k = 2; k <= 8; ++k) {
+                open[k] = INFINITY;
+                split[k] = 1;
+                for (int j = 1; j < k; ++j) {
+                    const float c = cost(nd.child[0], j, ca[0]) + cost(nd.child[1], k - j, ca[1]);
+                    if (c < open[k]) { open[k] = c; split[k] = (uint8_t)j; }
+                }
+            }
+            float* bv = &best[(size_t)v * 9];
+            uint8_t* hv = &how[(size_t)v * 9];
+            const float as_node = kNodeCost * av + open[8];
+            node_split[v] = split[8];
+            const float as_leaf = prims[v] <= 3 ? kLeafCost * av * (float)prims[v] : INFINITY;
+            bv[1] = std::min(as_leaf, as_node);
+            hv[1] = as_leaf <= as_node ? 0 : 1;
+            for (int k = 2; k <= 8; ++k) {
+                bv[k] = bv[k - 1];
+                hv[k] = hv[k - 1];
+                if (open[k] < bv[k]) { bv[k] = open[k]; hv[k] = (uint8_t)(2 + split[k]); }
+            }
+        }
+    }
+
+    // Triangles of a binary subtree, in leaf order.
+    void gather(int32_t code, std::vector<int32_t>& refs) const {
+        if (code < 0) {
+            const Leaf& l = t.leaves[-code - 2];
+            refs.insert(refs.end(), t.prim_refs.begin() + l.first, t.prim_refs.begin() + l.first + l.count);
+            return;
+        }
+        gather(t.nodes[code].child[0], refs);
+        gather(t.nodes[code].child[1], refs);
+    }
+
+    // The slots that the binary child `code` (box lo/hi) fills given k slots.
+    void slots(int32_t code, int k, const float* lo, const float* hi, std::vector<Child>& out) const {
+        if (code >= 0 && how[(size_t)code * 9 + k] >= 2) {
+            const TreeNode<2>& nd = t.nodes[code];
+            const int j = how[(size_t)code * 9 + k] - 2;
+            slots(nd.child[0], j, nd.lo[0], nd.hi[0], out);
+            slots(nd.child[1], k - j, nd.lo[1], nd.hi[1], out);
+            return;
+        }
+        out.push_back(Child{code, lo, hi});
+    }
+};
+}  // namespace
+
+static void collapse_optimal(const Tree<2>& t2, Tree<8>& out) {
+    Collapse cl(t2);
+    cl.run();
+    out = Tree<8>();
+    out.bounds = t2.bounds;
+    std::vector<std::pair<int32_t, int32_t>> work{{0, 0}};  // (binary node, 8-wide node)
+    out.nodes.push_back(TreeNode<8>{});
+    while (!work.empty()) {
+        const auto [src, dst] = work.back();
+        work.pop_back();
+        const TreeNode<2>& nd = t2.nodes[src];
+        const int j = cl.node_split[src];  // an 8-wide node opens its binary node into 8 slots
+        std::vector<Collapse::Child> ch;
+        cl.slots(nd.child[0], j, nd.lo[0], nd.hi[0], ch);
+        cl.slots(nd.child[1], 8 - j, nd.lo[1], nd.hi[1], ch);
+        TreeNode<8> d{};
+        for (int k = 0; k < 8; ++k) d.child[k] = -1;
+        d.count = (int)ch.size();
+        for (size_t c = 0; c < ch.size(); ++c) {
+            for (int a = 0; a < 3; ++a) { d.lo[c][a] = ch[c].lo[a]; d.hi[c][a] = ch[c].hi[a]; }
+            const int32_t code = ch[c].code;
+            if (code >= 0 && cl.how[(size_t)code * 9 + 1] == 1) {
+                const int32_t ni = (int32_t)out.nodes.size();
+                out.nodes.push_back(TreeNode<8>{});
+                work.push_back({code, ni});
+                d.child[c] = ni;
+            } else {
+                // A binary leaf, or a subtree merged into one leaf (<= 3 triangles).
+                const int32_t first = (int32_t)out.prim_refs.size();
+                cl.gather(code, out.prim_refs);
+                const int32_t leaf = (int32_t)out.leaves.size();
+                out.leaves.push_back(Leaf{first, (int32_t)out.prim_refs.size() - first});
+                d.child[c] = -(leaf + 2);
+            }
+        }
+        out.nodes[dst] = d;
+    }
+}
+
+
 void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out) {
     out = Tree<8>();
     out.bounds = t2.bounds;
@@ -289,58 +450,7 @@ void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out) {
         out.nodes.push_back(r);
         return;
     }
-    struct Item { int32_t src; int32_t dst; };
-    std::vector<Item> work;
-    out.nodes.reserve(t2.nodes.size() / 3 + 1);
-    out.nodes.push_back(TreeNode<8>{});
-    work.push_back({0, 0});
-    while (!work.empty()) {
-        const Item it = work.back();
-        work.pop_back();
-        const TreeNode<2>& s = t2.nodes[it.src];
-        int32_t code[8];
-        float lo[8][3], hi[8][3];
-        int cnt = 2;
-        for (int c = 0; c < 2; ++c) {
-            code[c] = s.child[c];
-            for (int a = 0; a < 3; ++a) { lo[c][a] = s.lo[c][a]; hi[c][a] = s.hi[c][a]; }
-        }
-        while (cnt < 8) {
-            int pick = -1;
-            float best = -1.f;
-            for (int c = 0; c < cnt; ++c) {
-                if (code[c] < 0) continue;
-                BBox b;
-                for (int a = 0; a < 3; ++a) { b.lo[a] = lo[c][a]; b.hi[a] = hi[c][a]; }
-                const float ar = b.area();
-                if (ar > best) { best = ar; pick = c; }
-            }
-            if (pick < 0) break;
-            const TreeNode<2>& o = t2.nodes[code[pick]];
-            code[pick] = o.child[0];
-            code[cnt] = o.child[1];
-            for (int a = 0; a < 3; ++a) {
-                lo[pick][a] = o.lo[0][a]; hi[pick][a] = o.hi[0][a];
-                lo[cnt][a] = o.lo[1][a];  hi[cnt][a] = o.hi[1][a];
-            }
-            ++cnt;
-        }
-        TreeNode<8> d{};
-        d.count = cnt;
-        for (int k = 0; k < 8; ++k) d.child[k] = -1;
-        for (int c = 0; c < cnt; ++c) {
-            for (int a = 0; a < 3; ++a) { d.lo[c][a] = lo[c][a]; d.hi[c][a] = hi[c][a]; }
-            if (code[c] < 0) {
-                d.child[c] = code[c];
-            } else {
-                const int32_t ni = (int32_t)out.nodes.size();
-                out.nodes.push_back(TreeNode<8>{});
-                d.child[c] = ni;
-                work.push_back({code[c], ni});
-            }
-        }
-        out.nodes[it.dst] = d;
-    }
+    collapse_optimal(t2, out);
 }
 
 template <int W>
