@@ -54,7 +54,9 @@ def workload_spec(name: str, quick: bool, rank: int):
     if quick:
         tris = np.minimum(tris, 200_000)
         rays = np.minimum(rays, 1 << 20)
-    return [dict(seed=i + 100 * rank, tris=int(t), rays=int(r), small=False) for i, (t, r) in enumerate(zip(tris, rays))]
+    from cwbvh_b200.replicas import rank_seed
+    return [dict(seed=rank_seed(i, rank), tris=int(t), rays=int(r), small=False)
+            for i, (t, r) in enumerate(zip(tris, rays))]
 
 
 def build_scenes(spec, threads_per_build: int = 1):
@@ -136,9 +138,8 @@ def time_steps(fn, steps: int, warmup: int, stream, dist=None, flush=None) -> fl
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        from cwbvh_b200.replicas import max_over_ranks
+        ms = max_over_ranks(ms, dist, device="cuda")
         dist.barrier()
     return ms
 

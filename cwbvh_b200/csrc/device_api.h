@@ -46,12 +46,7 @@ struct TraceItem {
     int64_t count;
     uint32_t node_f4;  // node buffer length in float4 (bounds checks)
     uint32_t woop_f4;  // Woop buffer length in float4
-    uint32_t flags;    // kItemFastSlab: see below
 };
-
-// The scene's coordinates are below 2^40 in magnitude and its node
-// exponents at most 38, so no slab value of a finite ray can be NaN.
-constexpr uint32_t kItemFastSlab = 1u;
 
 struct TraceParams {
     TraceItem single;         // the scene when the kernel is not a batch kernel

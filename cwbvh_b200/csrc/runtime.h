@@ -26,7 +26,6 @@ struct rq_scene {
     bool owned = false;
     float lo[3] = {0.f, 0.f, 0.f};
     float hi[3] = {0.f, 0.f, 0.f};
-    bool fast_slab = false;  // see kItemFastSlab
 };
 
 namespace rq {

@@ -25,13 +25,6 @@ namespace rq {
 
 constexpr int kStackTotal = 64;  // entries per lane (shared + local)
 
-// Build-time choices (kept selectable for measurement).
-#ifndef RQ_TRI_LAZY
-#define RQ_TRI_LAZY 1   // read Woop rows as the triangle test needs them
-#endif
-#ifndef RQ_FAST_SLAB
-#define RQ_FAST_SLAB 1  // float three-input min/max slab test where it decides exactly
-#endif
 #ifdef RQ_MAXNREG
 #define RQ_KERNEL_BOUNDS __maxnreg__(RQ_MAXNREG)  // register cap (occupancy experiments)
 #else
@@ -47,7 +40,6 @@ struct Lane {
     int64_t out_idx;
     int64_t gidx;
     uint32_t node_f4, woop_f4;
-    uint32_t flags;
 };
 
 template <bool MULTI>
@@ -67,7 +59,6 @@ __device__ __forceinline__ Ray fetch_ray(const TraceParams& p, int64_t g, Lane& 
     L.hits = it->hits;
     L.node_f4 = it->node_f4;
     L.woop_f4 = it->woop_f4;
-    L.flags = it->flags;
     L.out_idx = it->perm ? (int64_t)__ldg(it->perm + local) : local;
     L.gidx = g;
     Ray r;
@@ -84,16 +75,9 @@ __device__ __forceinline__ void store_hit(Hit* hits, int64_t i, float t, int add
 
 // Hit mask of the 8 children of one CWBVH node (src/TraversalKernelCWBVH.cu:
 // 141-288): bits 24-31 for inner children at 24 + (slot ^ octinv), the
-// unary triangle counts at their offsets for leaf children.
-//
-// EXACT: the slab extremes are taken as the reference does, on the float bits
-// compared as signed integers, then clamped by tmin / tmax with float
-// min/max.  FAST: plain float min/max with the three-input instructions.  For
-// a ray with tmin > 0 whose slab values are all non-NaN, both give the same
-// decision cmin <= cmax: cmin is positive either way and equal whenever some
-// entry value is non-negative (the integer order of non-negative floats is
-// the float order); a negative exit value makes cmax negative either way.
-template <bool FAST>
+// unary triangle counts at their offsets for leaf children.  The slab
+// extremes are taken as the reference does, on the float bits compared as
+// signed integers, then clamped by tmin / tmax with float min/max.
 __device__ __forceinline__ unsigned cwbvh_hitmask(const float4& n1, const float4& n2, const float4& n3,
                                                   const float4& n4, float adjx, float adjy, float adjz, float orx,
                                                   float ory, float orz, bool negx, bool negy, bool negz,
@@ -122,14 +106,8 @@ __device__ __forceinline__ unsigned cwbvh_hitmask(const float4& n1, const float4
             const float tx1 = __fmaf_rn(byte_to_float(hix, c), adjx, orx);
             const float ty1 = __fmaf_rn(byte_to_float(hiy, c), adjy, ory);
             const float tz1 = __fmaf_rn(byte_to_float(hiz, c), adjz, orz);
-            float cmin, cmax;
-            if (FAST) {
-                cmin = fmax3(tx0, ty0, fmaxf(tz0, tmin));
-                cmax = fmin3(tx1, ty1, fminf(tz1, tmax));
-            } else {
-                cmin = fmaxf(imax3(tx0, ty0, tz0), tmin);
-                cmax = fminf(imin3(tx1, ty1, tz1), tmax);
-            }
+            const float cmin = fmaxf(imax3(tx0, ty0, tz0), tmin);
+            const float cmax = fminf(imin3(tx1, ty1, tz1), tmax);
             if (cmin <= cmax) hitmask |= ((bits4 >> (8 * c)) & 0xFFu) << ((bitidx4 >> (8 * c)) & 0xFFu);
         }
     }
@@ -152,7 +130,7 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
     uint2 ng = make_uint2(0u, 0u), tg = make_uint2(0u, 0u);
     int sp = 0, hit_addr = -1, steps = 0, nvis = 0, ntri = 0;
     float hu = 0.f, hv = 0.f;
-    bool active = false, exhausted = false, lane_fast = false;
+    bool active = false, exhausted = false;
     const float rt = p.postpone_ratio;
 
     auto push = [&](uint2 v) -> bool {
@@ -199,11 +177,6 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
                     idz = guarded_rcp(dz);
                     octinv = 7u - (((dx < 0.f) ? 4u : 0u) | ((dy < 0.f) ? 2u : 0u) | ((dz < 0.f) ? 1u : 0u));
                     octinv4 = octinv * 0x01010101u;
-                    // Finite ray with tmin > 0 and origin below 2^40 in a fast-slab scene:
-                    // the float min/max slab test decides exactly as the integer one.
-                    lane_fast = (L.flags & kItemFastSlab) && tmin > 0.f && fabsf(ox) < 0x1p40f &&
-                                fabsf(oy) < 0x1p40f && fabsf(oz) < 0x1p40f && isfinite(dx) && isfinite(dy) &&
-                                isfinite(dz);
                     ng = make_uint2(0u, 0x80000000u);
                     tg = make_uint2(0u, 0u);
                     sp = 0; hit_addr = -1; hu = 0.f; hv = 0.f; steps = 0; nvis = 0; ntri = 0;
@@ -217,7 +190,6 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
 
         int lost = 0;
         for (;;) {
-            const bool warp_fast = RQ_FAST_SLAB && __all_sync(kFullMask, !active || lane_fast);
             // ---- node phase: take the nearest child of the current node group
             unsigned fault = 0u;
             if (active) {
@@ -244,11 +216,8 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
                         const float ory = __fmul_rn(-__fsub_rn(oy, n0.y), idy);
                         const float orz = __fmul_rn(-__fsub_rn(oz, n0.z), idz);
                         const bool negx = idx_ < 0.f, negy = idy < 0.f, negz = idz < 0.f;
-                        const unsigned hitmask =
-                            warp_fast ? cwbvh_hitmask<true>(n1, n2, n3, n4, adjx, adjy, adjz, orx, ory, orz, negx,
-                                                            negy, negz, octinv4, tmin, tmax)
-                                      : cwbvh_hitmask<false>(n1, n2, n3, n4, adjx, adjy, adjz, orx, ory, orz, negx,
-                                                             negy, negz, octinv4, tmin, tmax);
+                        const unsigned hitmask = cwbvh_hitmask(n1, n2, n3, n4, adjx, adjy, adjz, orx, ory, orz, negx,
+                                                               negy, negz, octinv4, tmin, tmax);
                         ng = make_uint2(__float_as_uint(n1.x), (hitmask & 0xFF000000u) | (ew >> 24));
                         tg = make_uint2(__float_as_uint(n1.y), hitmask & 0x00FFFFFFu);
                     }
@@ -281,13 +250,8 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
                             const float4* tp = L.woop + tri;
                             if (COUNT) ++ntri;
                             float t, u, v;
-#if RQ_TRI_LAZY
-                            const bool accept = woop_test_lazy(tp, ox, oy, oz, dx, dy, dz, tmin, tmax, t, u, v);
-#else
                             const float4 v0 = ld_nc(tp), v1 = ld_nc(tp + 1), v2 = ld_nc(tp + 2);
-                            const bool accept = woop_test(v0, v1, v2, ox, oy, oz, dx, dy, dz, tmin, tmax, t, u, v);
-#endif
-                            if (accept) {
+                            if (woop_test(v0, v1, v2, ox, oy, oz, dx, dy, dz, tmin, tmax, t, u, v)) {
                                 tmax = t;
                                 hit_addr = (int)tri;
                                 hu = u;

@@ -54,18 +54,6 @@ __device__ __forceinline__ float imax_then_min(float a, float b, float c) {
     return __int_as_float(min(max(__float_as_int(a), __float_as_int(b)), __float_as_int(c)));
 }
 
-// Three-input float max / min (sm_100 instructions).
-__device__ __forceinline__ float fmax3(float a, float b, float c) {
-    float r;
-    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-__device__ __forceinline__ float fmin3(float a, float b, float c) {
-    float r;
-    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
-    return r;
-}
-
 // 1/d with the 2^-80 guard against division by zero (src/TraversalKernelCWBVH.cu:78-80).
 __device__ __forceinline__ float guarded_rcp(float d) {
     return __frcp_rn(fabsf(d) > kOoeps ? d : copysignf(kOoeps, d));
@@ -86,29 +74,6 @@ __device__ __forceinline__ bool woop_test(const float4& v0, const float4& v1, co
     const float Dy = __fmaf_rn(dz, v2.z, __fmaf_rn(dx, v2.x, __fmul_rn(dy, v2.y)));
     v = __fmaf_rn(t, Dy, Oy);
     return (t > tmin && t < tmax) && (u >= 0.0f && u <= 1.0f) && (v >= 0.0f && __fadd_rn(u, v) <= 1.0f);
-}
-
-// The same test reading the rows as it needs them: V1 only when t is inside
-// (tmin, tmax), V2 only when u is inside [0, 1] (the order of the BVH2 kernel,
-// src/TraversalKernelBVH2.cu:135-151).  Same acceptance and, when accepted,
-// the same t, u, v as woop_test; a rejected triangle costs fewer loads.
-__device__ __forceinline__ bool woop_test_lazy(const float4* tp, float ox, float oy, float oz, float dx, float dy,
-                                               float dz, float tmin, float tmax, float& t, float& u, float& v) {
-    const float4 v0 = ld_nc(tp);
-    const float Oz = __fmaf_rn(-oz, v0.z, __fmaf_rn(-oy, v0.y, __fmaf_rn(-ox, v0.x, v0.w)));
-    const float Dz = __fmaf_rn(dz, v0.z, __fmaf_rn(dx, v0.x, __fmul_rn(dy, v0.y)));
-    t = __fmul_rn(Oz, __frcp_rn(Dz));
-    if (!(t > tmin && t < tmax)) return false;
-    const float4 v1 = ld_nc(tp + 1);
-    const float Ox = __fmaf_rn(oz, v1.z, __fmaf_rn(oy, v1.y, __fmaf_rn(ox, v1.x, v1.w)));
-    const float Dx = __fmaf_rn(dz, v1.z, __fmaf_rn(dx, v1.x, __fmul_rn(dy, v1.y)));
-    u = __fmaf_rn(t, Dx, Ox);
-    if (!(u >= 0.0f && u <= 1.0f)) return false;
-    const float4 v2 = ld_nc(tp + 2);
-    const float Oy = __fmaf_rn(oz, v2.z, __fmaf_rn(oy, v2.y, __fmaf_rn(ox, v2.x, v2.w)));
-    const float Dy = __fmaf_rn(dz, v2.z, __fmaf_rn(dx, v2.x, __fmul_rn(dy, v2.y)));
-    v = __fmaf_rn(t, Dy, Oy);
-    return v >= 0.0f && __fadd_rn(u, v) <= 1.0f;
 }
 
 // Exact float of an unsigned byte: 2^23 + b has b in its low mantissa bits.

@@ -64,8 +64,8 @@ typedef struct rq_launch {
     int blocks_per_sm;    /* persistent grid = SMs x this (0 = occupancy max)   */
     int smem_stack;       /* stack entries per lane in shared memory: 4, 8, 16  */
     float postpone_ratio; /* triangle postponing threshold Rt (reference 0.2)   */
-    int fetch_nd;         /* dynamic fetch: idle lanes tolerated (reference 4)  */
-    int fetch_nw;         /* dynamic fetch: lost-iteration budget (reference 16)*/
+    int fetch_nd;         /* dynamic fetch: idle lanes tolerated (default 0, reference 4)       */
+    int fetch_nw;         /* dynamic fetch: lost-iteration budget (default 1, reference 16)     */
 } rq_launch;
 
 /* --------------------------------------------------- host BVH construction */
