@@ -120,6 +120,11 @@ def test_oracle_matches_reference_kernels(rq, po, tag, kind):
     fx = np.load(GOLD / "trace_fixtures.npz")
     V, I, rays = fx["V"], fx["I"], fx["rays"]
     ref = fx[f"{tag}/ref_hits"]
+    # The reference's persistent CWBVH loop drops a few rays (never written,
+    # still the NaN pre-fill); they are excluded.
+    written = ~np.isnan(ref[:, 0])
+    assert written.mean() > 0.98
+    rays, ref = rays[written], ref[written]
     want = po.trace(kind, fx[f"{tag}/nodes"], fx[f"{tag}/woop"], rays, False)
     res = compare(po, rays, ref, want, fx[f"{tag}/prim"], V, I, any_hit=False)
     assert res["hits"] > rays.shape[0] // 10

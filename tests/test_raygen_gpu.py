@@ -78,7 +78,13 @@ def test_reference_generator_same_distribution(rq, po):
     lib.ref_cuda_free(C.c_void_p(p))
     ref = out.cpu().numpy()
     mine = rq.GenerateAORaysUniform(n, spp, pos, nrm, rad).cpu().numpy()
-    for r in (ref, mine):
+    # The reference's sqrtf(1 - x^2 - y^2) (src/ValidationKernels.cu:60) can
+    # see a tiny negative argument under -use_fast_math and return NaN; this
+    # generator clamps it at 0.
+    ref_finite = np.isfinite(ref[:, 4:7]).all(axis=1)
+    assert ref_finite.mean() > 0.99
+    assert np.isfinite(mine).all()
+    for r in (ref[ref_finite], mine):
         c = r[:, 4:7] @ np.array([0, 0.6, 0.8], np.float32)
         assert abs(c.mean() - 2 / 3) < 5e-3 and abs((c ** 2).mean() - 0.5) < 5e-3
     assert np.allclose(ref[:, 0:4], mine[:, 0:4], atol=1e-6)
