@@ -141,3 +141,4 @@ def check(status: int, where: str) -> None:
 
 
 _sig("rq_convert_tree", C.c_int, i32, i64, vp, vp, i64, vp, vp, i64, vp, i32, vp, i64, vp, i64, P(vp))
+_sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)

@@ -20,6 +20,8 @@ rq_status cuda_fail(cudaError_t e, const char* what) {
     return RQ_ERR_CUDA;
 }
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 int device_sms(int device) {
     static std::mutex mu;
     static std::map<int, int> cache;

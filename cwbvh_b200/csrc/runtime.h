@@ -32,6 +32,8 @@ namespace rq {
 
 // Records a failing CUDA call for rq_last_error and maps it to a status.
 rq_status cuda_fail(cudaError_t e, const char* what);
+// Sets the text rq_last_error returns on this thread.
+void set_last_error(const std::string& msg);
 
 #define RQ_CUDA(call)                                          \
     do {                                                       \

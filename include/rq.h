@@ -229,6 +229,23 @@ rq_status rq_sort_rays(rq_ctx_t ctx, const rq_ray* rays, int64_t count, const fl
                        const float bounds_hi[3], rq_ray* sorted_rays, int32_t* perm,
                        void* stream);
 
+/* rq_sort_rays without allocating device memory.  No counterpart in the
+ * reference.  Some callers cannot call cudaMalloc -- a plugin inside a host
+ * that owns all device memory through its own pool, code running while its
+ * host captures the stream into a CUDA graph, a service whose memory budget
+ * was fixed at start-up -- and rq_sort_rays allocates its sort buffers on
+ * every call.  This entry point keeps its scratch in one static 20 MiB device
+ * array that every GPU loading librq holds until exit, which limits a call to
+ * RQ_SORT_STATIC_MAX_RAYS rays (larger counts return RQ_ERR_INVALID_ARG with
+ * the limit in rq_last_error).  Outputs are identical to rq_sort_rays's.
+ * The first call on a device (with that device current) looks up the array's
+ * address; make it before any stream capture.  All calls share the array and
+ * leave their contents in it: calls whose work overlaps on the GPU race. */
+#define RQ_SORT_STATIC_MAX_RAYS 524288
+rq_status rq_sort_rays_static(const rq_ray* rays, int64_t count, const float bounds_lo[3],
+                              const float bounds_hi[3], rq_ray* sorted_rays, int32_t* perm,
+                              void* stream);
+
 /* -------------------------------------------------------------- batching */
 /*
  * A batch traces many (scene, rays, hits) items in one persistent launch over
