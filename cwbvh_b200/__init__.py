@@ -25,7 +25,8 @@ __all__ = [
     "trace", "trace_ordered", "trace_counted", "aorays", "sample_surfels", "ao_reduce", "sort_rays",
     "autotune", "autotune_batch", "default_launch", "woopify", "gen_heightfield_boxes", "gen_city",
     "gen_spheres_terrain", "rtBindCWBVHData", "rtTraceCWBVH", "rtBindBVH2Data", "rtTraceBVH2",
-    "rtOccludedCWBVH", "rtOccludedBVH2", "GenerateAORaysUniform", "version", "lib",
+    "rtOccludedCWBVH", "rtOccludedBVH2", "GenerateAORaysUniform", "version", "lib", "camera_rays",
+    "surfels_from_hits",
 ]
 
 
@@ -125,7 +126,7 @@ class HostBVH:
     """A converted BVH in host memory (node / Woop / primitive-index buffers)."""
 
     def __init__(self, vertices, indices, kind: int = CWBVH, max_leaf_size: int = 0, sah_bins: int = 0,
-                 max_depth: int = 0, threads: int = 0, tree: Optional[dict] = None):
+                 max_depth: int = 0, threads: int = 0, tree: Optional[dict] = None, presplit: int = 0):
         """Build with the library's SAH builder, or -- with `tree` (the dict
         shape of HostBVH.tree()) -- convert a tree built elsewhere."""
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
@@ -133,7 +134,7 @@ class HostBVH:
         self.vertices, self.indices, self.kind = v, i, kind
         h = C.c_void_p()
         if tree is None:
-            bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads)
+            bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads, presplit)
             check(lib.rq_build_bvh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0], kind, C.byref(bp),
                                    C.byref(h)), "rq_build_bvh")
         else:
@@ -317,6 +318,33 @@ def sample_surfels(vertices, indices, n: int, seed: int = 0, stream=None):
     nt = indices.numel() // 3
     check(lib.rq_sample_surfels(_ptr(vertices), _ptr(indices), nt, n, seed, _ptr(pos), _ptr(nrm), _ptr(rad),
                                 _stream(stream)), "rq_sample_surfels")
+    return pos, nrm, rad
+
+
+def camera_rays(eye, look, up, vfov_deg: float, width: int, height: int, tmin: float = 0.0, tmax: float = 1e20,
+                stream=None):
+    """Pinhole camera rays, one per pixel, row-major (a torch CUDA (w*h, 8) tensor)."""
+    import torch
+    with _On(stream):
+        out = torch.empty((width * height, 8), dtype=torch.float32, device="cuda")
+    f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])  # noqa: E731
+    check(lib.rq_camera_rays(f3(eye), f3(look), f3(up), vfov_deg, width, height, tmin, tmax, _ptr(out),
+                             _stream(stream)), "rq_camera_rays")
+    return out
+
+
+def surfels_from_hits(rays, hits, scene: "Scene", stream=None):
+    """Surfels at closest-hit points (facing geometric normals); misses get a zero normal."""
+    import torch
+    n = _rows(rays, 8, "rays")
+    if _rows(hits, 4, "hits") < n:
+        raise ValueError(f"hits: fewer than the {n} rows of rays")
+    with _On(stream):
+        pos = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        nrm = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+        rad = torch.empty((n,), dtype=torch.float32, device="cuda")
+    check(lib.rq_surfels_from_hits(scene._h, _ptr(rays), _ptr(hits), n, _ptr(pos), _ptr(nrm), _ptr(rad),
+                                   _stream(stream)), "rq_surfels_from_hits")
     return pos, nrm, rad
 
 

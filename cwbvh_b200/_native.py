@@ -47,7 +47,8 @@ class Launch(C.Structure):
 
 
 class BuildParams(C.Structure):
-    _fields_ = [("max_leaf_size", C.c_int), ("sah_bins", C.c_int), ("max_depth", C.c_int), ("threads", C.c_int)]
+    _fields_ = [("max_leaf_size", C.c_int), ("sah_bins", C.c_int), ("max_depth", C.c_int), ("threads", C.c_int),
+                ("presplit", C.c_int)]
 
 
 class BVHInfo(C.Structure):
@@ -142,3 +143,5 @@ def check(status: int, where: str) -> None:
 
 _sig("rq_convert_tree", C.c_int, i32, i64, vp, vp, i64, vp, vp, i64, vp, i32, vp, i64, vp, i64, P(vp))
 _sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)
+_sig("rq_camera_rays", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, f32, f32, vp, vp)
+_sig("rq_surfels_from_hits", C.c_int, vp, vp, vp, i64, vp, vp, vp, vp)

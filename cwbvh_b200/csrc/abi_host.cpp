@@ -58,13 +58,15 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
     if (nt > (int64_t)INT32_MAX / 3) return RQ_ERR_INVALID_ARG;
     for (int64_t k = 0; k < 3 * nt; ++k)
         if (indices[k] < 0 || indices[k] >= nv) return RQ_ERR_INVALID_ARG;
-    rq_build_params bp{4, 32, 30, 0};
+    rq_build_params bp{4, 32, 30, 0, 1};
     if (params) {
         if (params->max_leaf_size > 0) bp.max_leaf_size = params->max_leaf_size;
         if (params->sah_bins > 0) bp.sah_bins = params->sah_bins;
         if (params->max_depth > 0) bp.max_depth = params->max_depth;
         bp.threads = params->threads;
+        if (params->presplit > 0) bp.presplit = params->presplit;
     }
+    if (bp.presplit != 1 && bp.presplit != 2 && bp.presplit != 4 && bp.presplit != 8) return RQ_ERR_INVALID_ARG;
     rq_host_bvh* h = new (std::nothrow) rq_host_bvh();
     if (!h) return RQ_ERR_OOM;
     try {
@@ -73,12 +75,13 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
         m.i.assign(indices, indices + 3 * nt);
         h->b.kind = kind;
         if (kind == RQ_BVH_BVH2) {
-            build_bvh2_tree(m, std::max(1, bp.max_leaf_size), bp.sah_bins, bp.max_depth, true, bp.threads, h->b.tree2);
+            build_bvh2_tree(m, std::max(1, bp.max_leaf_size), bp.sah_bins, bp.max_depth, true, bp.threads, h->b.tree2,
+                            bp.presplit);
             convert_bvh2(h->b.tree2, m, h->b);
             h->b.depth = tree_depth2(h->b.tree2);
         } else {
             // The 8-wide tree's leaves hold at most 3 triangles (3 meta bits).
-            build_bvh2_tree(m, 3, bp.sah_bins, 48, false, bp.threads, h->b.tree2);
+            build_bvh2_tree(m, 3, bp.sah_bins, 48, false, bp.threads, h->b.tree2, bp.presplit);
             collapse_to_bvh8(h->b.tree2, h->b.tree8);
             convert_cwbvh(h->b.tree8, m, h->b);
             h->b.depth = tree_depth8(h->b.tree8);

@@ -72,8 +72,15 @@ struct Builder2 {
     std::atomic<int> spare_threads{0};
 
     int32_t make_leaf(int64_t begin, int64_t end) {
+        // Fragments of one split triangle can share a leaf: keep one of each.
+        int64_t n = 0;
+        for (int64_t k = begin; k < end; ++k) {
+            bool dup = false;
+            for (int64_t j = begin; j < begin + n; ++j) dup = dup || refs[j].id == refs[k].id;
+            if (!dup) refs[begin + n++] = refs[k];
+        }
         const int32_t l = n_leaves.fetch_add(1);
-        leaves[l] = Leaf{(int32_t)begin, (int32_t)(end - begin)};
+        leaves[l] = Leaf{(int32_t)begin, (int32_t)n};
         return -(l + 2);
     }
 
@@ -220,20 +227,82 @@ struct Builder2 {
 
 }  // namespace
 
-void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
-                     Tree<2>& out) {
-    Builder2 b;
+// ----------------------------------------------------------- pre-splitting --
+// A long thin triangle lying diagonally in its box (common in steep terrain)
+// has a box far larger than itself, and rays entering the box mostly miss
+// it.  Before the build such triangles are cut at the midplane of their box's
+// longest axis, recursively, into up to `max_frags` fragments; each fragment
+// is a reference to the same triangle with the bounds of the clipped polygon.
+// Triangles are taken worst fit first (box area / triangle area) until one
+// extra reference per triangle has been spent.  Leaves keep one reference per
+// triangle, so results are unchanged; only boxes get tighter.
+namespace {
+
+// Sutherland-Hodgman clip of a convex polygon to x[axis] <= pos (below) or
+// >= pos (above).
+int clip_polygon(const float (*in)[3], int n, int axis, float pos, bool below, float (*out)[3]) {
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+        const float* a = in[i];
+        const float* b = in[(i + 1) % n];
+        const float da = below ? pos - a[axis] : a[axis] - pos;
+        const float db = below ? pos - b[axis] : b[axis] - pos;
+        if (da >= 0.f) {
+            for (int k = 0; k < 3; ++k) out[m][k] = a[k];
+            ++m;
+        }
+        if ((da >= 0.f) != (db >= 0.f)) {
+            const float t = da / (da - db);
+            for (int k = 0; k < 3; ++k) out[m][k] = a[k] + t * (b[k] - a[k]);
+            out[m][axis] = pos;
+            ++m;
+        }
+    }
+    return m;
+}
+
+double tri_area(const Mesh& m, int64_t t) {
+    const V3 a = m.vert(m.i[3 * t]), b = m.vert(m.i[3 * t + 1]), c = m.vert(m.i[3 * t + 2]);
+    const V3 n = cross(b - a, c - a);
+    return 0.5 * std::sqrt((double)n.x * n.x + (double)n.y * n.y + (double)n.z * n.z);
+}
+
+void split_into(const float (*poly)[3], int n, const BBox& box, int frags, int32_t id, std::vector<PrimRef>& out) {
+    if (frags <= 1 || n == 0) {
+        if (n == 0) return;
+        PrimRef p{};
+        for (int a = 0; a < 3; ++a) { p.lo[a] = INFINITY; p.hi[a] = -INFINITY; }
+        for (int i = 0; i < n; ++i)
+            for (int a = 0; a < 3; ++a) { p.lo[a] = fmn(p.lo[a], poly[i][a]); p.hi[a] = fmx(p.hi[a], poly[i][a]); }
+        for (int a = 0; a < 3; ++a) {  // stay inside the parent box (clipping rounds)
+            p.lo[a] = fmx(p.lo[a], box.lo[a]);
+            p.hi[a] = fmn(p.hi[a], box.hi[a]);
+            if (p.lo[a] > p.hi[a]) p.lo[a] = p.hi[a];
+        }
+        p.id = id;
+        out.push_back(p);
+        return;
+    }
+    int axis = 0;
+    for (int a = 1; a < 3; ++a)
+        if (box.hi[a] - box.lo[a] > box.hi[axis] - box.lo[axis]) axis = a;
+    const float mid = 0.5f * (box.lo[axis] + box.hi[axis]);
+    float lp[12][3], rp[12][3];
+    const int nl = clip_polygon(poly, n, axis, mid, true, lp);
+    const int nr = clip_polygon(poly, n, axis, mid, false, rp);
+    BBox lb = box, rb = box;
+    lb.hi[axis] = mid;
+    rb.lo[axis] = mid;
+    split_into(lp, nl, lb, frags / 2, id, out);
+    split_into(rp, nr, rb, frags / 2, id, out);
+}
+
+std::vector<PrimRef> make_refs(const Mesh& m, int max_frags) {
     const int64_t nt = m.nt();
-    b.max_leaf = max_leaf;
-    b.big_leaves = big_leaves;
-    b.bins = std::max(2, std::min(bins, kMaxBins));
-    b.max_depth = max_depth;
-    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-    b.spare_threads = threads - 1;
-    b.refs.resize(nt);
-    BBox all, call;
+    std::vector<PrimRef> refs(nt);
+    std::vector<std::pair<float, int32_t>> fit;  // (box area / triangle area, triangle)
     for (int64_t t = 0; t < nt; ++t) {
-        PrimRef& p = b.refs[t];
+        PrimRef& p = refs[t];
         for (int a = 0; a < 3; ++a) { p.lo[a] = INFINITY; p.hi[a] = -INFINITY; }
         for (int k = 0; k < 3; ++k) {
             const float* v = &m.v[3 * (size_t)m.i[3 * t + k]];
@@ -241,6 +310,59 @@ void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool 
         }
         p.id = (int32_t)t;
         p.pad = 0;
+        if (max_frags > 1) {
+            BBox b;
+            b.grow(p.lo, p.hi);
+            const double at = tri_area(m, t);
+            if (at > 0.0) fit.push_back({(float)(b.area() / (2.0 * at)), (int32_t)t});
+        }
+    }
+    if (max_frags <= 1 || fit.empty()) return refs;
+    // Worst fit first; a box at most 4x the triangle's area is left alone.
+    std::sort(fit.begin(), fit.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+    int64_t budget = nt;
+    std::vector<PrimRef> extra;
+    std::vector<uint8_t> replaced(nt, 0);
+    for (const auto& [ratio, t] : fit) {
+        if (ratio <= 4.0f || budget <= 0) break;
+        float poly[3][3];
+        for (int k = 0; k < 3; ++k)
+            for (int a = 0; a < 3; ++a) poly[k][a] = m.v[3 * (size_t)m.i[3 * (int64_t)t + k] + a];
+        BBox b;
+        b.grow(refs[t].lo, refs[t].hi);
+        const size_t before = extra.size();
+        split_into(poly, 3, b, max_frags, t, extra);
+        const int64_t added = (int64_t)(extra.size() - before);
+        if (added <= 1) {
+            extra.resize(before);
+            continue;
+        }
+        replaced[t] = 1;
+        budget -= added - 1;
+    }
+    std::vector<PrimRef> out;
+    out.reserve(nt + extra.size());
+    for (int64_t t = 0; t < nt; ++t)
+        if (!replaced[t]) out.push_back(refs[t]);
+    out.insert(out.end(), extra.begin(), extra.end());
+    return out;
+}
+
+}  // namespace
+
+void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
+                     Tree<2>& out, int max_frags) {
+    Builder2 b;
+    b.max_leaf = max_leaf;
+    b.big_leaves = big_leaves;
+    b.bins = std::max(2, std::min(bins, kMaxBins));
+    b.max_depth = max_depth;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    b.spare_threads = threads - 1;
+    b.refs = make_refs(m, max_frags);
+    const int64_t nt = (int64_t)b.refs.size();
+    BBox all, call;
+    for (const PrimRef& p : b.refs) {
         float c[3];
         centroid(p, c);
         all.grow(p.lo, p.hi);
@@ -369,14 +491,19 @@ struct Collapse {
     }
 
     // Triangles of a binary subtree, in leaf order.
-    void gather(int32_t code, std::vector<int32_t>& refs) const {
+    // Triangles of a binary subtree appended to refs, each once from `first` on
+    // (fragments of one pre-split triangle can sit in sibling leaves).
+    void gather(int32_t code, std::vector<int32_t>& refs, size_t first) const {
         if (code < 0) {
             const Leaf& l = t.leaves[-code - 2];
-            refs.insert(refs.end(), t.prim_refs.begin() + l.first, t.prim_refs.begin() + l.first + l.count);
+            for (int32_t k = 0; k < l.count; ++k) {
+                const int32_t id = t.prim_refs[l.first + k];
+                if (std::find(refs.begin() + first, refs.end(), id) == refs.end()) refs.push_back(id);
+            }
             return;
         }
-        gather(t.nodes[code].child[0], refs);
-        gather(t.nodes[code].child[1], refs);
+        gather(t.nodes[code].child[0], refs, first);
+        gather(t.nodes[code].child[1], refs, first);
     }
 
     // The slots that the binary child `code` (box lo/hi) fills given k slots.
@@ -422,7 +549,7 @@ static void collapse_optimal(const Tree<2>& t2, Tree<8>& out) {
             } else {
                 // A binary leaf, or a subtree merged into one leaf (<= 3 triangles).
                 const int32_t first = (int32_t)out.prim_refs.size();
-                cl.gather(code, out.prim_refs);
+                cl.gather(code, out.prim_refs, (size_t)first);
                 const int32_t leaf = (int32_t)out.leaves.size();
                 out.leaves.push_back(Leaf{first, (int32_t)out.prim_refs.size() - first});
                 d.child[c] = -(leaf + 2);

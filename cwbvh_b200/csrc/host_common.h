@@ -104,8 +104,10 @@ struct HostBVH {
 };
 
 // Builders (builder.cpp)
+// max_frags > 1: pre-split badly fitting triangles into up to max_frags
+// references with clipped bounds (power of two).
 void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
-                     Tree<2>& out);
+                     Tree<2>& out, int max_frags = 1);
 void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out);
 int tree_depth2(const Tree<2>& t);
 int tree_depth8(const Tree<8>& t);

@@ -3,6 +3,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <cmath>
 
 #include "runtime.h"
 #include "trace_common.cuh"
@@ -55,6 +56,11 @@ __global__ void aorays_kernel(const float4* __restrict__ pos, const float4* __re
     const float3 p = f3(pos[s]);
     const float3 n = f3(nrm[s]);
     const float r = radius ? radius[s] : 0.0f;
+    if (n.x == 0.f && n.y == 0.f && n.z == 0.f) {  // no surface (a primary miss): an empty ray
+        out[i].origin_tmin = make_float4(p.x, p.y, p.z, 0.f);
+        out[i].dir_tmax = make_float4(0.f, 0.f, 1.f, 0.f);
+        return;
+    }
     float3 t1 = cross3(n, make_float3(0.f, 0.f, 1.f));
     if (len3(t1) < 0.1f) t1 = cross3(n, make_float3(0.f, 1.f, 0.f));
     t1 = norm3(t1);
@@ -101,6 +107,42 @@ __global__ void surfels_kernel(const float* __restrict__ v, const int32_t* __res
     const float3 nn = norm3(cross3(sub3(p1, p0), sub3(p2, p0)));
     pos[i] = make_float4(p.x, p.y, p.z, 1.0f);
     nrm[i] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+    if (radius) radius[i] = 0.0f;
+}
+
+// Pinhole camera: pixel (x, y) centre through an image plane at distance 1.
+__global__ void camera_rays_kernel(float3 eye, float3 fwd, float3 right, float3 upv, float half_w, float half_h,
+                                   int width, int height, float tmin, float tmax, Ray* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)width * height) return;
+    const int x = (int)(i % width), y = (int)(i / width);
+    const float sx = ((x + 0.5f) / width * 2.0f - 1.0f) * half_w;
+    const float sy = (1.0f - (y + 0.5f) / height * 2.0f) * half_h;
+    const float3 d = norm3(add3(add3(fwd, mul3(right, sx)), mul3(upv, sy)));
+    out[i].origin_tmin = make_float4(eye.x, eye.y, eye.z, tmin);
+    out[i].dir_tmax = make_float4(d.x, d.y, d.z, tmax);
+}
+
+// Hit point and facing geometric normal of each closest hit.
+__global__ void surfels_from_hits_kernel(const Ray* __restrict__ rays, const Hit* __restrict__ hits,
+                                         const float4* __restrict__ woop, int64_t woop_f4, int64_t n,
+                                         float4* __restrict__ pos, float4* __restrict__ nrm,
+                                         float* __restrict__ radius) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 o = rays[i].origin_tmin, d = rays[i].dir_tmax;
+    const float4 h = hits[i].t_triId_u_v;
+    const int addr = __float_as_int(h.y);
+    if (addr < 0 || addr >= woop_f4) {
+        pos[i] = make_float4(o.x, o.y, o.z, 1.0f);
+        nrm[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        const float4 v0 = __ldg(woop + addr);  // V0 = triangle-space z row: normal to the triangle
+        float3 nn = norm3(make_float3(v0.x, v0.y, v0.z));
+        if (nn.x * d.x + nn.y * d.y + nn.z * d.z > 0.f) nn = mul3(nn, -1.0f);
+        pos[i] = make_float4(o.x + h.x * d.x, o.y + h.x * d.y, o.z + h.x * d.z, 1.0f);
+        nrm[i] = make_float4(nn.x, nn.y, nn.z, 0.f);
+    }
     if (radius) radius[i] = 0.0f;
 }
 
@@ -271,6 +313,47 @@ rq_status rq_sample_surfels(const float* vertices, const int32_t* indices, int64
     if (n_surfels == 0) return RQ_OK;
     surfels_kernel<<<blocks_for(n_surfels, 256), 256, 0, (cudaStream_t)stream>>>(
         vertices, indices, nt, n_surfels, (uint32_t)seed, (uint32_t)(seed >> 32), (float4*)out_pos, (float4*)out_nrm,
+        out_radius);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+rq_status rq_camera_rays(const float eye[3], const float look[3], const float up[3], float vfov_deg, int width,
+                         int height, float tmin, float tmax, rq_ray* out_rays, void* stream) {
+    if (!eye || !look || !up || width <= 0 || height <= 0 || !(vfov_deg > 0.f && vfov_deg < 180.f) || !out_rays)
+        return RQ_ERR_INVALID_ARG;
+    // Camera frame on the host (once per call).
+    auto norm = [](float3 a) {
+        const float l = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+        return make_float3(a.x / l, a.y / l, a.z / l);
+    };
+    auto cross = [](float3 a, float3 b) {
+        return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+    };
+    auto len = [](float3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); };
+    const float3 e = make_float3(eye[0], eye[1], eye[2]);
+    const float3 view = make_float3(look[0] - eye[0], look[1] - eye[1], look[2] - eye[2]);
+    if (!(len(view) > 0.f) || !std::isfinite(len(view))) return RQ_ERR_INVALID_ARG;
+    const float3 fwd = norm(view);
+    const float3 side = cross(fwd, make_float3(up[0], up[1], up[2]));
+    if (!(len(side) > 1e-6f) || !std::isfinite(len(side))) return RQ_ERR_INVALID_ARG;  // up parallel to the view
+    const float3 right = norm(side);
+    const float3 upv = cross(right, fwd);
+    const float half_h = std::tan(vfov_deg * 0.5f * 3.14159265358979f / 180.0f);
+    const float half_w = half_h * (float)width / (float)height;
+    const int64_t n = (int64_t)width * height;
+    camera_rays_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(e, fwd, right, upv, half_w, half_h, width,
+                                                                             height, tmin, tmax, (Ray*)out_rays);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+rq_status rq_surfels_from_hits(const rq_scene* scene, const rq_ray* rays, const rq_hit* hits, int64_t count,
+                               float* out_pos, float* out_nrm, float* out_radius, void* stream) {
+    if (!scene || count < 0 || (count > 0 && (!rays || !hits || !out_pos || !out_nrm))) return RQ_ERR_INVALID_ARG;
+    if (count == 0) return RQ_OK;
+    surfels_from_hits_kernel<<<blocks_for(count, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const Ray*)rays, (const Hit*)hits, scene->woop, scene->woop_f4, count, (float4*)out_pos, (float4*)out_nrm,
         out_radius);
     RQ_CUDA(cudaGetLastError());
     return RQ_OK;

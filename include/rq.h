@@ -84,6 +84,8 @@ typedef struct rq_build_params {
     int sah_bins;         /* binned-SAH bins per axis (default 32)                         */
     int max_depth;        /* BVH2 depth limit (default 30; the reference stack is 32)      */
     int threads;          /* builder threads (0 = hardware concurrency)                    */
+    int presplit;         /* 1, 2, 4 or 8: cut badly fitting triangles into up to this     */
+                          /* many references with clipped boxes before the build (0 = 1)   */
 } rq_build_params;
 
 typedef struct rq_bvh_info {
@@ -215,6 +217,22 @@ rq_status rq_aorays(const float* pos, const float* nrm, const float* radius, int
 rq_status rq_sample_surfels(const float* vertices, const int32_t* indices, int64_t nt,
                             int64_t n_surfels, uint64_t seed, float* out_pos, float* out_nrm,
                             float* out_radius, void* stream);
+
+/* Pinhole camera rays, one per pixel centre, row-major (row 0 at the top):
+ * eye, look-at point, up vector, vertical field of view in degrees. */
+rq_status rq_camera_rays(const float eye[3], const float look[3], const float up[3], float vfov_deg,
+                         int width, int height, float tmin, float tmax, rq_ray* out_rays,
+                         void* stream);
+
+/* Surfels at closest-hit points (hit position o + t d, geometric normal from
+ * the hit triangle's Woop row V0 -- perpendicular to the triangle -- turned
+ * to face the incoming ray, radius 0).  A miss gives a zero normal, for which
+ * rq_aorays emits an empty ray (tmin = tmax = 0).  hits must come from a
+ * closest-hit trace of this scene; a hit address outside its Woop buffer is
+ * treated as a miss. */
+rq_status rq_surfels_from_hits(const rq_scene* scene, const rq_ray* rays, const rq_hit* hits,
+                               int64_t count, float* out_pos, float* out_nrm, float* out_radius,
+                               void* stream);
 
 /* Per-surfel AO fraction (occluded rays / spp) from any-hit results whose rays
  * were generated surfel-major (ray i belongs to surfel i / spp). */

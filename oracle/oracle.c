@@ -318,6 +318,12 @@ void oracle_aorays(const float* pos, const float* nrm, const float* radius, int6
         const float p[3] = {pos[4 * s], pos[4 * s + 1], pos[4 * s + 2]};
         const float nn[3] = {nrm[4 * s], nrm[4 * s + 1], nrm[4 * s + 2]};
         const float r = radius ? radius[s] : 0.0f;
+        if (nn[0] == 0.f && nn[1] == 0.f && nn[2] == 0.f) {  /* no surface: an empty ray */
+            float* o = out + 8 * i;
+            o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; o[3] = 0.f;
+            o[4] = 0.f; o[5] = 0.f; o[6] = 1.f; o[7] = 0.f;
+            continue;
+        }
         float t1[3] = {nn[1] * 1.0f - nn[2] * 0.0f, nn[2] * 0.0f - nn[0] * 1.0f, nn[0] * 0.0f - nn[1] * 0.0f};
         if (sqrtf(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]) < 0.1f) {
             t1[0] = nn[1] * 0.0f - nn[2] * 1.0f;

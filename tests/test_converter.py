@@ -168,6 +168,35 @@ def test_convert_tree_rejects_bad_trees(rq):
         rq.HostBVH(V, I, tree=bad)
 
 
+@pytest.mark.parametrize("presplit", [2, 4, 8])
+def test_presplit_keeps_results(rq, po, presplit):
+    """Pre-split references change boxes only: every ray gets the same
+    occlusion bit and closest triangle, and each leaf lists a triangle once."""
+    from cwbvh_b200 import workloads as W
+    from adjudicate import prim_ids
+    V, I = W.heightfield_boxes(1, grid=24, n_boxes=40)
+    rng = np.random.default_rng(4)
+    n = 20000
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(-0.1, 1.1, (n, 3))
+    d = rng.normal(size=(n, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3], rays[:, 7] = 1e-4, 0.3
+    base = rq.HostBVH(V, I, rq.CWBVH)
+    split = rq.HostBVH(V, I, rq.CWBVH, presplit=presplit)
+    tr = split.tree()
+    for f, c in zip(tr["leaf_first"], tr["leaf_count"]):
+        ids = tr["prim_refs"][f:f + c]
+        assert len(set(ids.tolist())) == c
+    assert set(tr["prim_refs"].tolist()) == set(range(I.shape[0]))
+    for any_hit in (False, True):
+        a = prim_ids(po.trace(0, base.nodes, base.woop, rays, any_hit), base.prim_index)
+        b = prim_ids(po.trace(0, split.nodes, split.woop, rays, any_hit), split.prim_index)
+        assert np.array_equal(a >= 0, b >= 0)
+        if not any_hit:
+            assert np.array_equal(a, b)
+
+
 def test_builder_invariants(rq):
     """Leaves hold <= 3 triangles (CWBVH), every triangle is referenced once,
     and the depth stays within the traversal stacks."""

@@ -107,6 +107,16 @@ def test_aorays_cosine_lobe(po):
         assert (r[:, 3] == np.float32(0.01)).all() and (r[:, 7] == np.float32(1e20)).all()
 
 
+def test_aorays_zero_normal_is_empty_ray(po):
+    """A surfel without a surface (a primary miss) yields empty rays:
+    origin at the surfel, tmin = tmax = 0, so no traversal can report a hit."""
+    pos = np.array([[1, 2, 3, 1], [4, 5, 6, 1]], np.float32)
+    nrm = np.array([[0, 0, 0, 0], [0, 0, 1, 0]], np.float32)
+    r = po.aorays(pos, nrm, np.array([0.5, 0.5], np.float32), 3, 5, 0.01, 9.0, 1.0)
+    assert np.array_equal(r[:3], np.tile(np.array([1, 2, 3, 0, 0, 0, 1, 0], np.float32), (3, 1)))
+    assert (r[3:, 3] == np.float32(0.01)).all() and (r[3:, 7] == np.float32(9.0)).all()
+
+
 def test_adjudicator_f64(po):
     ray = np.array([0.25, 0.25, -1, 0, 0, 0, 1, 10], np.float32)
     t, u, v, det = po.tri_f64(ray, [1, 0, 0], [0, 1, 0], [0, 0, 0])
