@@ -129,14 +129,29 @@ def time_steps(fn, steps: int, warmup: int, stream, dist=None, flush=None) -> fl
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        fn()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+    if flush is None:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+    else:
+        # inputs smaller than L2: write `flush` (larger than L2) before each
+        # step, outside the events, so every step starts from a cold L2
+        evs = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.add_(1)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / steps
     if dist is not None:
         from cwbvh_b200.replicas import max_over_ranks
         ms = max_over_ranks(ms, dist, device="cuda")
@@ -150,6 +165,24 @@ def measured_peak_hbm():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def measure_l2_read(stream, mbytes: int = 48, reps: int = 100) -> float:
+    """L2 read bandwidth (GB/s) from the library's probe kernel
+    (rq_probe_l2_read): a 48 MB buffer, well inside the 126 MB L2, read
+    `reps` times with L1-bypassing 16-byte loads."""
+    import torch
+    import cwbvh_b200 as rq
+    n = mbytes << 20
+    with torch.cuda.stream(stream):
+        buf = torch.ones(n // 4, dtype=torch.int32, device="cuda")
+        sink = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def run():
+        rq.check(rq.lib.rq_probe_l2_read(buf.data_ptr(), n, reps, sink.data_ptr(), stream.cuda_stream),
+                 "rq_probe_l2_read")
+    ms = time_steps(run, 5, 3, stream)
+    return n * reps / (ms * 1e-3) / 1e9
 
 
 def profile_traffic(workload: str):
@@ -211,7 +244,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rq", choices=["rq", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "small"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "small", "city", "large"])
+    ap.add_argument("--rays", type=int, default=0, help="large: total AO rays (default 64M; 16M with --quick)")
     ap.add_argument("--quick", action="store_true", help="8 smaller scenes (smoke runs)")
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
@@ -238,6 +272,13 @@ def main():
 
     import cwbvh_b200 as rq
     from cwbvh_b200 import workloads as W
+
+    if args.workload in ("city", "large"):
+        (run_city if args.workload == "city" else run_large)(args, world, rank, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     spec = workload_spec(args.workload, args.quick, rank)
     t0 = time.time()
@@ -266,7 +307,11 @@ def main():
         for ds, r, h in zip(scenes, rays, hits):
             rq.trace(ctx, ds.scene, r, h, rq.ANY, stream=stream)
 
-    ms_plain = time_steps(plain, args.steps, warmup, stream, dist)
+    flush = None
+    if args.workload == "small":  # 1M rays + hits (48 MB) fit in L2
+        with torch.cuda.stream(stream):
+            flush = torch.zeros(64 << 20, dtype=torch.int32, device="cuda")  # 256 MB > 126 MB L2
+    ms_plain = time_steps(plain, args.steps, warmup, stream, dist, flush)
     ctx.check(stream)
     plain_occ = [h[:, 1].view(torch.int32).ne(-1).sum().item() for h in hits]
 
@@ -277,7 +322,7 @@ def main():
     log(f"[bench] autotune {time.time()-t0:.1f}s -> block {bp.launch.block_size} smem {bp.launch.smem_stack} "
         f"sort_threshold {bp.sort_threshold} graph {bp.use_graph}")
     batch = rq.Batch(ctx, items, rq.ANY, params=bp)
-    ms_batch = time_steps(lambda: batch.run(stream), args.steps, warmup, stream, dist)
+    ms_batch = time_steps(lambda: batch.run(stream), args.steps, warmup, stream, dist, flush)
     ctx.check(stream)
     batch_occ = [h[:, 1].view(torch.int32).ne(-1).sum().item() for h in hits]
     occlusion_identical = plain_occ == batch_occ
@@ -285,7 +330,7 @@ def main():
     # trace kernel alone (the dominant kernel) for the roofline
     batch.run(stream)
     ms_kernel = time_steps(lambda: rq.lib.rq_batch_run_stage(batch._h, 2, stream.cuda_stream), args.steps, warmup,
-                           stream, dist)
+                           stream, dist, flush)
     ms_sort = time_steps(lambda: rq.lib.rq_batch_run_stage(batch._h, 1, stream.cuda_stream), 3, 1, stream, dist)
     launches_per_step = int(rq.lib.rq_batch_kernel_count(batch._h))
 
@@ -352,11 +397,17 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
     traffic = profile_traffic(args.workload)
+    l2_gbs = measure_l2_read(stream)
 
     # ---- the reference's CWBVH kernel rebuilt for sm_100a, same rays (closest-hit: its only mode)
     ref_gpu = None
     if not args.no_ref_gpu:
-        ref_gpu = run_ref_gpu(scenes, rays, warmup=1, steps=2)
+        ref_gpu, _ = run_ref_gpu(scenes, rays, warmup=1, steps=2)
+
+    # ---- the plain config's per-kernel table: CWBVH and BVH2, any-hit and closest-hit, + the reference's BVH2
+    kernels = None
+    if args.workload == "small":
+        kernels = run_small_kernels(args, built, scenes, rays, stream, ctx, dist, warmup, flush)
 
     # ---- serving configuration (continuous batching vs one request per launch)
     serving = None
@@ -398,7 +449,8 @@ def main():
             "layout": "CWBVH 80 B nodes, Woop 48 B triangles, Ray 32 B, Hit 16 B",
             "launch": {"block": bp.launch.block_size, "smem_stack": bp.launch.smem_stack,
                        "sort_threshold": int(bp.sort_threshold), "cuda_graph": bool(bp.use_graph)},
-            "l2": "inputs larger than L2 (rays+hits %.1f GB per step)" % (total_rays * 48 / 1e9),
+            "l2": ("inputs larger than L2 (rays+hits %.1f GB per step)" % (total_rays * 48 / 1e9)) if flush is None
+            else "L2 flushed before every timed step (256 MB write outside the events; rays+hits are 48 MB)",
             "parallelism": f"replicas x{world} (rays independent, no data-path collective)",
         },
         "plain_per_scene": {"value": round(world_rays / (ms_plain * 1e-3) / 1e6, 2), "unit": "Mrays/s",
@@ -420,13 +472,18 @@ def main():
                      "algorithmic_bytes_per_launch": int(alg_bytes),
                      "bytes_per_ray": round(alg_bytes / total_rays, 1),
                      "nodes_per_ray": round(nodes_total / total_rays, 3),
-                     "tris_per_ray": round(tris_total / total_rays, 3)},
+                     "tris_per_ray": round(tris_total / total_rays, 3),
+                     "l2": {"peak": round(l2_gbs, 1), "frac": round(achieved / l2_gbs, 4),
+                            "peak_source": "rq_probe_l2_read: 48 MB L2-resident buffer, 16 B L1-bypassing loads, "
+                                           "measured in this run"}},
         "gpu_launches": int(launches_per_step * args.steps),
         "clocks": clocks,
         "clocks_ms_per_step": round(ms_batch2, 4),
     }
     if serving is not None:
         line["serving"] = serving
+    if kernels is not None:
+        line["kernels"] = kernels
     if ref_gpu is not None:
         line["reference_cwbvh_kernel_sm100a"] = ref_gpu
         if ref_gpu.get("value"):
@@ -560,22 +617,28 @@ def run_serving(n_requests: int = 160, seed: int = 4242, rates=(0.25, 0.5, 0.75)
     }
 
 
-def run_ref_gpu(scenes, rays, warmup: int, steps: int):
-    """The reference's rtTraceCWBVH (oracle/_ref, compiled from its sources for
-    sm_100a, shipped 32x32x(32x2) grid) on the same scenes and rays."""
+def run_ref_gpu(scenes, rays, warmup: int, steps: int, kind: int = 0):
+    """The reference's rtTraceCWBVH (kind 0) or rtTraceBVH2 (kind 1)
+    (oracle/_ref, compiled from its sources for sm_100a, shipped grids) on the
+    same scenes and rays."""
     import torch
     try:
         from oracle import pyoracle as po
         if not po.ref_available():
-            return {"unavailable": "oracle/_ref/libref.so not built"}
+            return {"unavailable": "oracle/_ref/libref.so not built"}, None
         lib = po.ref()
     except Exception as e:  # pragma: no cover
-        return {"unavailable": str(e)}
+        return {"unavailable": str(e)}, None
     # The reference kernel has a 40-entry stack without an overflow check; a
     # tree of depth d needs at most 2d entries.
+    # The BVH2 kernel's stack holds 32 entries (a tree of depth d needs d).
     deepest = max(ds.host.info["depth"] for ds in scenes)
-    if 2 * deepest > 40:
-        return {"unavailable": f"tree depth {deepest} could overflow the reference's 40-entry stack"}
+    if kind == 0 and 2 * deepest > 40:
+        return {"unavailable": f"tree depth {deepest} could overflow the reference's 40-entry stack"}, None
+    if kind == 1 and deepest > 31:
+        return {"unavailable": f"tree depth {deepest} could overflow the reference's 32-entry stack"}, None
+    bind, trace = (lib.ref_bind_cwbvh, lib.ref_trace_cwbvh) if kind == 0 else (lib.ref_bind_bvh2, lib.ref_trace_bvh2)
+    tag = "rtTraceCWBVH" if kind == 0 else "rtTraceBVH2"
     import re
     import tempfile
     out_hits = [torch.empty((r.shape[0], 4), device="cuda") for r in rays]
@@ -589,8 +652,8 @@ def run_ref_gpu(scenes, rays, warmup: int, steps: int):
         def step():
             for ds, r, h in zip(scenes, rays, out_hits):
                 dn, dw, dp = C_buffers(ds.scene)
-                lib.ref_bind_cwbvh(dn, dw, dp)
-                lib.ref_trace_cwbvh(r.data_ptr(), h.data_ptr(), r.shape[0])
+                bind(dn, dw, dp)
+                trace(r.data_ptr(), h.data_ptr(), r.shape[0])
         for _ in range(warmup):
             step()
         torch.cuda.synchronize()
@@ -605,15 +668,15 @@ def run_ref_gpu(scenes, rays, warmup: int, steps: int):
     tmp.seek(0)
     txt = tmp.read().decode(errors="replace")
     tmp.close()
-    per_call = [float(m) for m in re.findall(r"([0-9.]+)MS, [0-9.]+MRays/s \(rtTraceCWBVH", txt)]
+    per_call = [float(m) for m in re.findall(r"([0-9.]+)MS, [0-9.]+MRays/s \(" + tag, txt)]
     timed = per_call[len(per_call) - steps * len(rays):] if len(per_call) >= steps * len(rays) else []
     ms = sum(timed) / steps if timed else wall_ms
     return {"value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
             "wall_ms_per_step": round(wall_ms, 3),
             "query": "closest-hit (the reference has no any-hit kernel)",
-            "timing": "sum of the reference's own CUDA-event kernel times (its log line per rtTraceCWBVH call)"
-            if timed else "host wall clock around synchronous rtTraceCWBVH calls",
-            "grid": "32x32 blocks of 32x2 threads (as shipped)"}
+            "timing": f"sum of the reference's own CUDA-event kernel times (its log line per {tag} call)"
+            if timed else f"host wall clock around synchronous {tag} calls",
+            "grid": "as shipped (CWBVH 32x32 blocks of 32x2 threads)"}, [h for h in out_hits]
 
 
 def C_buffers(scene):
@@ -643,6 +706,223 @@ def cpu_baseline(spec, built):
     return {"value": round(n / dt / 1e6, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
             "sample": f"{n} AO any-hit rays drawn from all scenes in proportion to their ray counts, CWBVH, "
                       f"oracle/oracle.c with OpenMP over {threads} threads, {dt:.1f}s"}
+
+
+def run_small_kernels(args, built, scenes, rays, stream, ctx, dist, warmup, flush):
+    """Plain launches of both kernel families on the plain config's scene and
+    rays (CWBVH and BVH2, any-hit and closest-hit), and the reference's BVH2
+    kernel (closest-hit) on the same rays."""
+    import torch
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+    V, I, _ = built[0]
+    r = rays[0]
+    hb2 = rq.HostBVH(V, I, rq.BVH2)
+    with torch.cuda.stream(stream):
+        sc2 = rq.Scene.from_host(hb2)
+        h = torch.empty((r.shape[0], 4), device="cuda")
+    out = {}
+    for sc, nm in ((scenes[0].scene, "cwbvh"), (sc2, "bvh2")):
+        for q, qn in ((rq.ANY, "any"), (rq.CLOSEST, "closest")):
+            ms = time_steps(lambda: rq.trace(ctx, sc, r, h, q, stream=stream), args.steps, warmup, stream, dist,
+                            flush)
+            out[f"{nm}_{qn}"] = {"mrays_per_s": round(r.shape[0] / (ms * 1e-3) / 1e6, 2), "ms": round(ms, 4)}
+    ctx.check(stream)
+    if not args.no_ref_gpu:
+        ds2 = W.DeviceScene(rq.BVH2, hb2, sc2, None, None, W.diag(V), I.shape[0])
+        out["reference_bvh2_kernel_sm100a"], _ = run_ref_gpu([ds2], [r], 1, 3, kind=1)
+    return out
+
+
+def _counted_bytes(ctx, scene, rays, query, stream):
+    """Algorithmic bytes of one CWBVH pass: 32 + 16 per ray, 80 per node
+    fetched, 48 per triangle tested (counts from rq_trace_counted)."""
+    import torch
+    import cwbvh_b200 as rq
+    with torch.cuda.stream(stream):
+        hh = torch.empty((rays.shape[0], 4), device="cuda")
+        nv, nt = rq.trace_counted(ctx, scene, rays, hh, query, stream=stream)
+        nodes = int(nv.sum(dtype=torch.int64).item())
+        tris = int(nt.sum(dtype=torch.int64).item())
+        del hh, nv, nt
+    return 48 * int(rays.shape[0]) + 80 * nodes + 48 * tris, nodes, tris
+
+
+def _pass(name, n_rays, ms, alg=None, peak=None, l2=None):
+    d = {"rays": int(n_rays), "ms": round(ms, 4), "mrays_per_s": round(n_rays / (ms * 1e-3) / 1e6, 2)}
+    if alg is not None:
+        b, nodes, tris = alg
+        gbs = b / (ms * 1e-3) / 1e9
+        d.update({"bytes_per_ray": round(b / n_rays, 1), "nodes_per_ray": round(nodes / n_rays, 3),
+                  "tris_per_ray": round(tris / n_rays, 3), "achieved_gbs": round(gbs, 1)})
+        if peak:
+            d["hbm_frac"] = round(gbs / peak, 4)
+        if l2:
+            d["l2_frac"] = round(gbs / l2, 4)
+    return d
+
+
+def _single_line(args, world, warmup, workload: str, value: float, ms: float, extra: dict):
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene; the reference's mesh.dat/samplecache.dat are not shipped)",
+            "config": {"workload": workload, "l2": "inputs larger than L2",
+                       "parallelism": f"replicas x{world} (rays independent, no data-path collective)"}}
+    line.update(extra)
+    return line
+
+
+def run_city(args, world, rank, dist):
+    """Single mid-size scene: a 1M-triangle city (10k box/prism buildings,
+    log-normal heights, ground grid), 4096x4096 pinhole primary rays
+    closest-hit, then one AO any-hit ray per primary hit (tmax = 0.05 diag).
+    The passes are reported separately and combined."""
+    import torch
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+    warmup = max(3, args.warmup)
+    t0 = time.time()
+    V, I = rq.gen_city(rank, 10000)
+    hb = rq.HostBVH(V, I, rq.CWBVH)
+    log(f"[bench] city {I.shape[0]/1e6:.2f}M tris built in {time.time()-t0:.1f}s")
+    stream = torch.cuda.Stream()
+    ctx = rq.Context()
+    with torch.cuda.stream(stream):
+        sc = rq.Scene.from_host(hb)
+    dg = W.diag(V)
+    lo, hi = V.min(0), V.max(0)
+    ext = hi - lo
+    eye = (float(lo[0] - 0.05 * ext[0]), float(lo[1] - 0.05 * ext[1]), float(0.25 * max(ext[0], ext[1])))
+    look = (float(0.5 * (lo[0] + hi[0])), float(0.5 * (lo[1] + hi[1])), 0.0)
+    w = h = 2048 if args.quick else 4096
+    n = w * h
+    prim = rq.camera_rays(eye, look, (0.0, 0.0, 1.0), 60.0, w, h, 0.0, 10.0 * dg, stream=stream)
+    with torch.cuda.stream(stream):
+        ph = torch.empty((n, 4), device="cuda")
+    ms_prim = time_steps(lambda: rq.trace(ctx, sc, prim, ph, rq.CLOSEST, stream=stream), args.steps, warmup,
+                         stream, dist)
+    out = {}
+
+    def gen():
+        pos, nrm, rad = rq.surfels_from_hits(prim, ph, sc, stream=stream)
+        out["ao"] = rq.aorays(pos, nrm, rad, 1, seed=rank + 77, tmin=1e-4 * dg, tmax=0.05 * dg, offset_scale=0.0,
+                              stream=stream)
+    ms_gen = time_steps(gen, args.steps, warmup, stream, dist)
+    ao = out["ao"]
+    with torch.cuda.stream(stream):
+        ah = torch.empty((n, 4), device="cuda")
+    ms_ao = time_steps(lambda: rq.trace(ctx, sc, ao, ah, rq.ANY, stream=stream), args.steps, warmup, stream, dist)
+    # the same AO rays Morton-sorted inside a one-item batch (sort + trace + scatter of hits)
+    sah = torch.empty((n, 4), device="cuda")
+    sb = rq.Batch(ctx, [(sc, ao, sah)], rq.ANY, sort_threshold=0, use_graph=True)
+    ms_ao_sorted = time_steps(lambda: sb.run(stream), args.steps, warmup, stream, dist)
+    ctx.check(stream)
+    torch.cuda.synchronize()
+    hit_frac = float((ph[:, 1].view(torch.int32) >= 0).float().mean().item())
+    occ = float((ah[:, 1].view(torch.int32) != -1).float().mean().item())
+    same = bool(torch.equal(ah[:, 1].view(torch.int32) != -1, sah[:, 1].view(torch.int32) != -1))
+    peak, peak_kind = measured_peak_hbm()
+    l2 = measure_l2_read(stream)
+    a_prim = _counted_bytes(ctx, sc, prim, rq.CLOSEST, stream)
+    a_ao = _counted_bytes(ctx, sc, ao, rq.ANY, stream)
+    ref = {}
+    if not args.no_ref_gpu:
+        ref, ref_hits = run_ref_gpu([W.DeviceScene(rq.CWBVH, hb, sc, None, None, dg, I.shape[0])], [prim], 1, 2)
+        if ref_hits:
+            mine = ph[:, 1].view(torch.int32)
+            theirs = ref_hits[0][:, 1].view(torch.int32)
+            pm = torch.from_numpy(hb.prim_index).cuda()
+            pid = lambda a: torch.where(a >= 0, pm[a.clamp(min=0).long()], torch.full_like(a, -1))  # noqa: E731
+            ref["closest_prim_ids_equal_frac"] = round(float((pid(mine) == pid(theirs)).float().mean().item()), 6)
+    total = 2 * n
+    ms_total = ms_prim + ms_gen + ms_ao
+    extra = {
+        "passes": {"primary_closest": _pass("primary", n, ms_prim, a_prim, peak, l2),
+                   "ao_raygen": {"ms": round(ms_gen, 4), "what": "surfels_from_hits + aorays (1 spp)"},
+                   "ao_any": _pass("ao", n, ms_ao, a_ao, peak, l2),
+                   "ao_any_morton_sorted": _pass("ao_sorted", n, ms_ao_sorted)},
+        "primary_hit_fraction": round(hit_frac, 4), "ao_occluded_fraction": round(occ, 4),
+        "ao_sorted_occlusion_identical": same,
+        "triangles": int(I.shape[0]), "image": f"{w}x{h}",
+        "roofline": {"bound": "hbm", "achieved": _pass("", n, ms_ao, a_ao)["achieved_gbs"], "peak": peak,
+                     "unit": "GB/s", "frac": _pass("", n, ms_ao, a_ao, peak)["hbm_frac"],
+                     "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                     "l2": {"peak": round(l2, 1), "frac": _pass("", n, ms_ao, a_ao, None, l2)["l2_frac"]},
+                     "kernel": "AO any-hit pass"},
+    }
+    if ref:
+        extra["reference_cwbvh_kernel_sm100a_primary"] = ref
+    line = _single_line(args, world, warmup, f"city: {I.shape[0]/1e6:.2f}M tris, {w}x{h} primary closest-hit "
+                        "+ 1 AO any-hit ray per primary hit (tmax 0.05 diag); value = both passes + raygen",
+                        world * total / (ms_total * 1e-3) / 1e6, ms_total, extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_large(args, world, rank, dist):
+    """Single large scene: displaced subdivided spheres + terrain tiles
+    (30M triangles; 3M with --quick), 16M surfels x 4 spp = 64M incoherent
+    AO any-hit rays (tmin 1e-4 diag, tmax 0.1 diag), unsorted vs
+    Morton-sorted; the scene is far larger than L2, so node fetches go to HBM."""
+    import torch
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+    warmup = max(3, args.warmup)
+    n_tris = 3_000_000 if args.quick else 30_000_000
+    n_surf = (1 << 22) if args.quick else (1 << 24)
+    if args.rays:
+        n_surf = max(1, args.rays // 4)
+    spp = 4
+    t0 = time.time()
+    V, I = rq.gen_spheres_terrain(rank, n_tris)
+    hb = rq.HostBVH(V, I, rq.CWBVH)
+    log(f"[bench] large {I.shape[0]/1e6:.1f}M tris built in {time.time()-t0:.1f}s "
+        f"(nodes {hb.nodes.nbytes/1e9:.2f} GB, woop {hb.woop.nbytes/1e9:.2f} GB)")
+    stream = torch.cuda.Stream()
+    ctx = rq.Context()
+    with torch.cuda.stream(stream):
+        sc = rq.Scene.from_host(hb)
+        v = torch.from_numpy(V).cuda()
+        i = torch.from_numpy(I).cuda()
+        pos, nrm, rad = rq.sample_surfels(v, i, n_surf, seed=rank + 1000, stream=stream)
+        dg = W.diag(V)
+        rays = rq.aorays(pos, nrm, rad, spp, seed=rank + 2000, tmin=1e-4 * dg, tmax=0.1 * dg, offset_scale=0.0,
+                         stream=stream)
+        del pos, nrm, rad, v, i
+        n = rays.shape[0]
+        hits = torch.empty((n, 4), device="cuda")
+        shits = torch.empty((n, 4), device="cuda")
+    ms_plain = time_steps(lambda: rq.trace(ctx, sc, rays, hits, rq.ANY, stream=stream), args.steps, warmup, stream,
+                          dist)
+    sb = rq.Batch(ctx, [(sc, rays, shits)], rq.ANY, sort_threshold=0, use_graph=True)
+    ms_sorted = time_steps(lambda: sb.run(stream), args.steps, warmup, stream, dist)
+    ms_sort = time_steps(lambda: rq.lib.rq_batch_run_stage(sb._h, 1, stream.cuda_stream), 3, 1, stream, dist)
+    ms_sorted_kernel = time_steps(lambda: rq.lib.rq_batch_run_stage(sb._h, 2, stream.cuda_stream), args.steps,
+                                  warmup, stream, dist)
+    ctx.check(stream)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(hits[:, 1].view(torch.int32) != -1, shits[:, 1].view(torch.int32) != -1))
+    occ = float((hits[:, 1].view(torch.int32) != -1).float().mean().item())
+    peak, peak_kind = measured_peak_hbm()
+    alg = _counted_bytes(ctx, sc, rays, rq.ANY, stream)
+    unsorted = _pass("unsorted", n, ms_plain, alg, peak)
+    best = min(ms_plain, ms_sorted)
+    extra = {
+        "passes": {"unsorted": unsorted,
+                   "morton_sorted": dict(_pass("sorted", n, ms_sorted), sort_ms=round(ms_sort, 4),
+                                         trace_kernel_ms=round(ms_sorted_kernel, 4))},
+        "sorted_occlusion_identical": same, "ao_occluded_fraction": round(occ, 4),
+        "triangles": int(I.shape[0]), "scene_bytes": int(hb.nodes.nbytes + hb.woop.nbytes),
+        "roofline": {"bound": "hbm", "achieved": unsorted["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": unsorted["hbm_frac"], "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                     "kernel": "unsorted AO any-hit trace"},
+    }
+    line = _single_line(args, world, warmup, f"large: {I.shape[0]/1e6:.1f}M tris, {n_surf} surfels x {spp} spp "
+                        "AO any-hit, unsorted vs Morton-sorted; value = the faster", world * n / (best * 1e-3) / 1e6,
+                        best, extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_reference(args, world, rank, warmup):

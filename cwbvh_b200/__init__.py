@@ -26,7 +26,7 @@ __all__ = [
     "autotune", "autotune_batch", "default_launch", "woopify", "gen_heightfield_boxes", "gen_city",
     "gen_spheres_terrain", "rtBindCWBVHData", "rtTraceCWBVH", "rtBindBVH2Data", "rtTraceBVH2",
     "rtOccludedCWBVH", "rtOccludedBVH2", "GenerateAORaysUniform", "version", "lib", "camera_rays",
-    "surfels_from_hits",
+    "surfels_from_hits", "load_mesh_dat", "save_mesh_dat", "load_samplecache_dat", "save_samplecache_dat",
 ]
 
 
@@ -112,6 +112,55 @@ def gen_spheres_terrain(seed: int = 0, target_tris: int = 1_000_000):
     return _take_mesh(v, nv, i, nt)
 
 
+def load_mesh_dat(path):
+    """(vertices (nV, 3) float32, indices (nT, 3) int32, materials (nT,) int32)
+    from the reference's mesh.dat format."""
+    v, i, m, nv, nt = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_int64(), C.c_int64()
+    check(lib.rq_load_mesh_dat(str(path).encode(), C.byref(v), C.byref(nv), C.byref(i), C.byref(nt), C.byref(m)),
+          "rq_load_mesh_dat")
+    mats = np.ctypeslib.as_array(C.cast(m, C.POINTER(C.c_int32)), shape=(nt.value,)).copy() if nt.value else \
+        np.zeros(0, np.int32)
+    lib.rq_free_host(m)
+    verts, idx = _take_mesh(v, nv, i, nt)
+    return verts, idx, mats
+
+
+def save_mesh_dat(path, vertices, indices, materials=None) -> None:
+    v = np.ascontiguousarray(vertices, np.float32).reshape(-1, 3)
+    i = np.ascontiguousarray(indices, np.int32).reshape(-1, 3)
+    m = None if materials is None else np.ascontiguousarray(materials, np.int32).reshape(-1)
+    if m is not None and m.size != i.shape[0]:
+        raise ValueError("materials: one per triangle")
+    check(lib.rq_save_mesh_dat(str(path).encode(), v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0],
+                               None if m is None else m.ctypes.data), "rq_save_mesh_dat")
+
+
+def load_samplecache_dat(path):
+    """(size_x, size_y, pos (n, 4), nrm (n, 4), radius (n,)) from the
+    reference's samplecache.dat format, n = size_x * size_y."""
+    sx, sy, p, q, r = C.c_int32(), C.c_int32(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    check(lib.rq_load_samplecache_dat(str(path).encode(), C.byref(sx), C.byref(sy), C.byref(p), C.byref(q),
+                                      C.byref(r)), "rq_load_samplecache_dat")
+    n = sx.value * sy.value
+    take = lambda ptr, k: (np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(k,)).copy()  # noqa: E731
+                           if k else np.zeros(0, np.float32))
+    out = (sx.value, sy.value, take(p, 4 * n).reshape(-1, 4), take(q, 4 * n).reshape(-1, 4), take(r, n))
+    for ptr in (p, q, r):
+        lib.rq_free_host(ptr)
+    return out
+
+
+def save_samplecache_dat(path, size_x: int, size_y: int, pos, nrm, radius) -> None:
+    n = size_x * size_y
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 4)
+    q = np.ascontiguousarray(nrm, np.float32).reshape(-1, 4)
+    r = np.ascontiguousarray(radius, np.float32).reshape(-1)
+    if p.shape[0] != n or q.shape[0] != n or r.size != n:
+        raise ValueError(f"sample cache arrays must hold size_x * size_y = {n} entries")
+    check(lib.rq_save_samplecache_dat(str(path).encode(), size_x, size_y, p.ctypes.data, q.ctypes.data,
+                                      r.ctypes.data), "rq_save_samplecache_dat")
+
+
 def woopify(v0, v1, v2) -> np.ndarray:
     """3 float4 Woop rows (V0, V1, V2) of one triangle, shape (3, 4)."""
     a = [np.ascontiguousarray(x, dtype=np.float32) for x in (v0, v1, v2)]
@@ -148,6 +197,9 @@ class HostBVH:
                                       lf.size, lf.ctypes.data, lc.ctypes.data, refs.size, refs.ctypes.data,
                                       int(tree["root_is_leaf"]), v.ctypes.data, v.shape[0], i.ctypes.data,
                                       i.shape[0], C.byref(h)), "rq_convert_tree")
+        self._adopt(h)
+
+    def _adopt(self, h) -> None:
         self._h = h
         info = N.BVHInfo()
         check(lib.rq_host_bvh_info(h, C.byref(info)), "rq_host_bvh_info")
@@ -162,6 +214,21 @@ class HostBVH:
                      .copy().reshape(-1, 4) if info.woop_float4s else np.zeros((0, 4), np.float32))
         self.prim_index = (np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int32)), shape=(info.prim_index_count,))
                            .copy() if info.prim_index_count else np.zeros(0, np.int32))
+
+    def save(self, path) -> None:
+        """Write the converted buffers to a scene file (rq_host_bvh_save)."""
+        check(lib.rq_host_bvh_save(self._h, str(path).encode()), "rq_host_bvh_save")
+
+    @classmethod
+    def load(cls, path) -> "HostBVH":
+        """A host BVH from a scene file: buffers only, no builder tree, no mesh."""
+        h = C.c_void_p()
+        check(lib.rq_host_bvh_load(str(path).encode(), C.byref(h)), "rq_host_bvh_load")
+        self = cls.__new__(cls)
+        self.vertices = self.indices = None
+        self._adopt(h)
+        self.kind = self.info["kind"]
+        return self
 
     def tree(self) -> dict:
         """The pre-conversion tree (see rq_host_bvh_tree)."""

@@ -145,3 +145,11 @@ _sig("rq_convert_tree", C.c_int, i32, i64, vp, vp, i64, vp, vp, i64, vp, i32, vp
 _sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)
 _sig("rq_camera_rays", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, f32, f32, vp, vp)
 _sig("rq_surfels_from_hits", C.c_int, vp, vp, vp, i64, vp, vp, vp, vp)
+_sig("rq_probe_l2_read", C.c_int, vp, i64, C.c_int, vp, vp)
+_sig("rq_load_mesh_dat", C.c_int, cp, P(vp), P(i64), P(vp), P(i64), P(vp))
+_sig("rq_save_mesh_dat", C.c_int, cp, vp, i64, vp, i64, vp)
+_sig("rq_load_samplecache_dat", C.c_int, cp, P(i32), P(i32), P(vp), P(vp), P(vp))
+_sig("rq_save_samplecache_dat", C.c_int, cp, i32, i32, vp, vp, vp)
+_sig("rq_free_host", None, vp)
+_sig("rq_host_bvh_save", C.c_int, vp, cp)
+_sig("rq_host_bvh_load", C.c_int, cp, P(vp))

