@@ -26,7 +26,7 @@ __all__ = [
     "autotune", "autotune_batch", "default_launch", "woopify", "gen_heightfield_boxes", "gen_city",
     "gen_spheres_terrain", "rtBindCWBVHData", "rtTraceCWBVH", "rtBindBVH2Data", "rtTraceBVH2",
     "rtOccludedCWBVH", "rtOccludedBVH2", "GenerateAORaysUniform", "version", "lib", "camera_rays",
-    "surfels_from_hits", "load_mesh_dat", "save_mesh_dat", "load_samplecache_dat", "save_samplecache_dat",
+    "surfels_from_hits", "trace_ao", "load_mesh_dat", "save_mesh_dat", "load_samplecache_dat", "save_samplecache_dat",
 ]
 
 
@@ -347,6 +347,23 @@ def trace_ordered(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stre
     """Trace in the oracle's traversal order (bit-identical results)."""
     check(lib.rq_trace_ordered(ctx._h, scene._h, _ptr(rays), _ptr(hits), _rows(rays, 8, "rays"), query,
                                _stream(stream)), "rq_trace_ordered")
+
+
+def trace_ao(ctx: Context, scene: Scene, rays, spp: int, occluded=None, launch: Optional[Launch] = None,
+             stream=None):
+    """Fused AO bake (rq_trace_ao): per-surfel occluded-ray counts (int32
+    tensor, rays surfel-major with `spp` per surfel); AO = counts / spp.
+    `occluded`, if given, is accumulated into."""
+    import torch
+    n = _rows(rays, 8, "rays")
+    if spp <= 0 or n % spp:
+        raise ValueError(f"{n} rays are not a whole number of surfels of {spp} rays")
+    if occluded is None:
+        with _On(stream):
+            occluded = torch.zeros(n // spp, dtype=torch.int32, device=rays.device)
+    check(lib.rq_trace_ao(ctx._h, scene._h, _ptr(rays), n, spp, _ptr(occluded),
+                          C.byref(launch) if launch is not None else None, _stream(stream)), "rq_trace_ao")
+    return occluded
 
 
 def trace_counted(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stream=None):

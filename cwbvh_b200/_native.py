@@ -153,3 +153,4 @@ _sig("rq_save_samplecache_dat", C.c_int, cp, i32, i32, vp, vp, vp)
 _sig("rq_free_host", None, vp)
 _sig("rq_host_bvh_save", C.c_int, vp, cp)
 _sig("rq_host_bvh_load", C.c_int, cp, P(vp))
+_sig("rq_trace_ao", C.c_int, vp, vp, vp, i64, C.c_int, vp, P(Launch), vp)

@@ -60,6 +60,8 @@ struct TraceParams {
     int fetch_nd;
     int fetch_nw;
     int bvh2_speculative;
+    uint32_t* ao_counts;      // non-null: add occluded rays per surfel instead of writing hits
+    int ao_spp;               // rays per surfel (consecutive) when ao_counts is set
 };
 
 typedef void (*TraceKernelFn)(TraceParams);

@@ -321,8 +321,8 @@ rq_status rq_default_launch(rq_bvh_kind kind, rq_query query, rq_launch* out) {
 
 static rq_status trace_impl(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits, int64_t count,
                             rq_query query, const rq_launch* launch, int32_t* nv, int32_t* nt, int speculative,
-                            void* stream) {
-    if (!ctx || !scene || count < 0 || (count > 0 && (!rays || !hits))) return RQ_ERR_INVALID_ARG;
+                            void* stream, uint32_t* ao_counts = nullptr, int ao_spp = 0) {
+    if (!ctx || !scene || count < 0 || (count > 0 && (!rays || (!hits && !ao_counts)))) return RQ_ERR_INVALID_ARG;
     if (query != RQ_CLOSEST && query != RQ_ANY) return RQ_ERR_INVALID_ARG;
     if (count == 0) return RQ_OK;
     const rq_launch l = resolve_launch(scene->kind, query, launch);
@@ -333,6 +333,8 @@ static rq_status trace_impl(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, 
     p.total_rays = count;
     p.node_visits = nv;
     p.tri_tests = nt;
+    p.ao_counts = ao_counts;
+    p.ao_spp = ao_spp;
     if (speculative >= 0) p.bvh2_speculative = speculative;
     cudaStream_t s = (cudaStream_t)stream;
     rq_status st = reset_counter(ctx, s);
@@ -351,6 +353,12 @@ rq_status rq_trace_counted(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, r
     rq_launch l{};
     l.postpone_ratio = -1.0f;  // the oracle's order, so the counts are comparable per ray
     return trace_impl(ctx, scene, rays, hits, count, query, &l, node_visits, tri_tests, 0, stream);
+}
+
+rq_status rq_trace_ao(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, int64_t count, int spp,
+                      uint32_t* occluded, const rq_launch* launch, void* stream) {
+    if (spp <= 0 || count < 0 || count % spp != 0 || (count > 0 && !occluded)) return RQ_ERR_INVALID_ARG;
+    return trace_impl(ctx, scene, rays, nullptr, count, RQ_ANY, launch, nullptr, nullptr, -1, stream, occluded, spp);
 }
 
 // Trace with the traversal order of the CPU oracle: no triangle postponing

@@ -149,7 +149,11 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
             atomicOr(&p.scratch->error, err);
             hit_addr = -1;
         }
-        store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
+        if (p.ao_counts) {
+            if (hit_addr >= 0) atomicAdd(p.ao_counts + L.out_idx / p.ao_spp, 1u);
+        } else {
+            store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
+        }
         if (COUNT) {
             p.node_visits[L.gidx] = nvis;
             p.tri_tests[L.gidx] = ntri;
@@ -314,7 +318,11 @@ __global__ void RQ_KERNEL_BOUNDS bvh2_kernel(const TraceParams p) {
             atomicOr(&p.scratch->error, err);
             hit_addr = -1;
         }
-        store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
+        if (p.ao_counts) {
+            if (hit_addr >= 0) atomicAdd(p.ao_counts + L.out_idx / p.ao_spp, 1u);
+        } else {
+            store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
+        }
         if (COUNT) {
             p.node_visits[L.gidx] = nvis;
             p.tri_tests[L.gidx] = ntri;

@@ -186,6 +186,17 @@ rq_status rq_trace_counted(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, r
                            int64_t count, rq_query query, int32_t* node_visits,
                            int32_t* tri_tests, void* stream);
 
+/* AO bake in one pass (the per-surfel reduction fused into the trace
+ * epilogue): any-hit traversal of `count` rays laid out surfel-major (`spp`
+ * consecutive rays per surfel, as rq_aorays and GenerateAORaysUniform write
+ * them) that adds 1 to occluded[ray / spp] for each occluded ray instead of
+ * writing a Hit -- no 16-byte hit store per ray and no separate reduction.
+ * `occluded` (device, count / spp entries) accumulates: zero it for a fresh
+ * bake.  count must be a multiple of spp.  AO = occluded / spp, equal to
+ * rq_ao_reduce over rq_trace any-hit results. */
+rq_status rq_trace_ao(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, int64_t count, int spp,
+                      uint32_t* occluded, const rq_launch* launch, void* stream);
+
 /* rq_trace with the traversal order of the CPU oracle: no triangle
  * postponing (CWBVH) and no speculative leaf postponing (BVH2).  Its results
  * are bit-identical to the oracle's (t, id, u, v), which is what the parity

@@ -100,3 +100,30 @@ def test_ao_reduce(rq):
     ao = rq.ao_reduce(hits, n, spp).cpu().numpy()
     want = (ids.cpu().numpy().reshape(n, spp) != -1).mean(axis=1)
     assert np.allclose(ao, want)
+
+
+@pytest.mark.parametrize("kind", [0, 1], ids=["cwbvh", "bvh2"])
+def test_trace_ao_fused_equals_trace_then_reduce(rq, kind):
+    """rq_trace_ao (counts in the trace epilogue, no hit buffer) equals
+    any-hit rq_trace followed by rq_ao_reduce, surfel by surfel."""
+    import torch
+    from cwbvh_b200 import workloads as W
+    V, I = W.heightfield_boxes(2)
+    ds = W.upload(V, I, kind)
+    spp = 8
+    rays = W.ao_rays(ds, 40_000 * spp, seed=21, spp=spp)
+    ctx = rq.Context()
+    hits = torch.empty((rays.shape[0], 4), device="cuda")
+    rq.trace(ctx, ds.scene, rays, hits, rq.ANY)
+    want = rq.ao_reduce(hits, rays.shape[0] // spp, spp)
+    counts = rq.trace_ao(ctx, ds.scene, rays, spp)
+    ctx.check()
+    assert torch.equal(counts.float() / spp, want)
+    assert 0 < int(counts.sum()) < rays.shape[0]
+    rq.trace_ao(ctx, ds.scene, rays, spp, occluded=counts)  # accumulates
+    assert torch.equal(counts.float() / (2 * spp), want)
+    with pytest.raises(ValueError):
+        rq.trace_ao(ctx, ds.scene, rays[:-1], spp)
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        rq.check(rq.lib.rq_trace_ao(ctx._h, ds.scene._h, rays.data_ptr(), rays.shape[0] - 1, spp,
+                                    counts.data_ptr(), None, None), "rq_trace_ao")
