@@ -410,7 +410,7 @@ def main():
     alg_bytes = 48 * total_rays + 80 * nodes_total + 48 * tris_total
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
-    traffic = profile_traffic(args.workload)
+    traffic = profile_traffic(args.workload + ("_quick" if args.quick else ""))
     l2_gbs = measure_l2_read(stream)
 
     # ---- the reference's CWBVH kernel rebuilt for sm_100a, same rays (closest-hit: its only mode)
