@@ -244,7 +244,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="rq", choices=["rq", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "small", "city", "large"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "small", "city", "large", "instanced"])
     ap.add_argument("--rays", type=int, default=0, help="large: total AO rays (default 64M; 16M with --quick)")
     ap.add_argument("--quick", action="store_true", help="8 smaller scenes (smoke runs)")
     ap.add_argument("--no-ref-gpu", action="store_true")
@@ -275,8 +275,8 @@ def main():
     import cwbvh_b200 as rq
     from cwbvh_b200 import workloads as W
 
-    if args.workload in ("city", "large"):
-        (run_city if args.workload == "city" else run_large)(args, world, rank, dist)
+    if args.workload in ("city", "large", "instanced"):
+        {"city": run_city, "large": run_large, "instanced": run_instanced}[args.workload](args, world, rank, dist)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
@@ -870,6 +870,101 @@ def run_city(args, world, rank, dist):
     line = _single_line(args, world, warmup, f"city: {I.shape[0]/1e6:.2f}M tris, {w}x{h} primary closest-hit "
                         "+ 1 AO any-hit ray per primary hit (tmax 0.05 diag); value = both passes + raygen",
                         world * total / (ms_total * 1e-3) / 1e6, ms_total, extra)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_instanced(args, world, rank, dist):
+    """Two-level city: 64 block templates (16 buildings each, from the city
+    generator) placed 625 times on a 25 x 25 grid with quarter-turn rotations
+    (10,000 buildings) under a top-level CWBVH, against the same city
+    flattened into one mesh: 4096x4096 primary closest-hit and one AO any-hit
+    ray per primary hit through both."""
+    import torch
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+    warmup = max(3, args.warmup)
+    rng = np.random.default_rng(77 + rank)
+    templates = [rq.gen_city(1000 + i, 16) for i in range(64)]
+    blas = [rq.HostBVH(V, I, rq.CWBVH) for V, I in templates]
+    side, block = 25, 80.0
+    n_inst = side * side
+    bi = rng.integers(0, len(templates), n_inst).astype(np.int32)
+    M = np.zeros((n_inst, 3, 4), np.float32)
+    Vs, Is, nv = [], [], 0
+    for k in range(n_inst):
+        r = int(rng.integers(0, 4))
+        c, s_ = [(1, 0), (0, 1), (-1, 0), (0, -1)][r]
+        R = np.array([[c, -s_, 0], [s_, c, 0], [0, 0, 1]], np.float64)
+        ctr = np.array([block / 2, block / 2, 0.0])
+        off = np.array([(k % side) * block, (k // side) * block, 0.0])
+        M[k, :, :3] = R
+        M[k, :, 3] = off + ctr - R @ ctr
+        V, I = templates[bi[k]]
+        Vs.append((V.astype(np.float64) @ R.T + M[k, :, 3].astype(np.float64)).astype(np.float32))
+        Is.append(I + nv)
+        nv += V.shape[0]
+    FV, FI = np.concatenate(Vs), np.concatenate(Is).astype(np.int32)
+    t0 = time.time()
+    fhb = rq.HostBVH(FV, FI, rq.CWBVH)
+    log(f"[bench] instanced city: {n_inst} instances of {len(templates)} blocks; flat {FI.shape[0]/1e6:.2f}M tris "
+        f"built in {time.time()-t0:.1f}s")
+    stream = torch.cuda.Stream()
+    ctx = rq.Context()
+    with torch.cuda.stream(stream):
+        scenes = [rq.Scene.from_host(h) for h in blas]
+        flat = rq.Scene.from_host(fhb)
+    tlas = rq.Tlas(scenes, M, bi)
+    top = tlas.buffers()
+    inst_bytes = sum(h.nodes.nbytes + h.woop.nbytes for h in blas) + top["nodes"].nbytes + top["rows"].nbytes
+    flat_bytes = fhb.nodes.nbytes + fhb.woop.nbytes
+    dg = W.diag(FV)
+    lo, hi = FV.min(0), FV.max(0)
+    ext = hi - lo
+    eye = (float(lo[0] - 0.05 * ext[0]), float(lo[1] - 0.05 * ext[1]), float(0.25 * max(ext[0], ext[1])))
+    look = (float(0.5 * (lo[0] + hi[0])), float(0.5 * (lo[1] + hi[1])), 0.0)
+    w = h = 2048 if args.quick else 4096
+    n = w * h
+    prim = rq.camera_rays(eye, look, (0.0, 0.0, 1.0), 60.0, w, h, 0.0, 10.0 * dg, stream=stream)
+    with torch.cuda.stream(stream):
+        fh = torch.empty((n, 4), device="cuda")
+        ih = torch.empty((n, 4), device="cuda")
+        ii = torch.empty(n, dtype=torch.int32, device="cuda")
+    ms_flat_p = time_steps(lambda: rq.trace(ctx, flat, prim, fh, rq.CLOSEST, stream=stream), args.steps, warmup,
+                           stream, dist)
+    ms_inst_p = time_steps(lambda: rq.trace_instanced(ctx, tlas, prim, ih, rq.CLOSEST, ii, stream=stream),
+                           args.steps, warmup, stream, dist)
+    pos, nrm, rad = rq.surfels_from_hits(prim, fh, flat, stream=stream)
+    ao = rq.aorays(pos, nrm, rad, 1, seed=rank + 78, tmin=1e-4 * dg, tmax=0.05 * dg, offset_scale=0.0, stream=stream)
+    with torch.cuda.stream(stream):
+        fa = torch.empty((n, 4), device="cuda")
+        ia = torch.empty((n, 4), device="cuda")
+    ms_flat_a = time_steps(lambda: rq.trace(ctx, flat, ao, fa, rq.ANY, stream=stream), args.steps, warmup, stream,
+                           dist)
+    ms_inst_a = time_steps(lambda: rq.trace_instanced(ctx, tlas, ao, ia, rq.ANY, None, stream=stream), args.steps,
+                           warmup, stream, dist)
+    ctx.check(stream)
+    torch.cuda.synchronize()
+    fhit = fh[:, 1].view(torch.int32) >= 0
+    ihit = ih[:, 1].view(torch.int32) >= 0
+    tdiff = (fh[:, 0] - ih[:, 0]).abs() / fh[:, 0].abs().clamp(min=1e-30)
+    both = fhit & ihit
+    occ_same = float(((fa[:, 1].view(torch.int32) != -1) == (ia[:, 1].view(torch.int32) != -1)).float().mean())
+    total_ms = ms_inst_p + ms_inst_a
+    extra = {
+        "passes": {"primary_closest": {"instanced": _pass("", n, ms_inst_p), "flattened": _pass("", n, ms_flat_p)},
+                   "ao_any": {"instanced": _pass("", n, ms_inst_a), "flattened": _pass("", n, ms_flat_a)}},
+        "agreement": {"primary_hit_same_frac": round(float((fhit == ihit).float().mean()), 6),
+                      "primary_t_rel_p999": round(float(tdiff[both].float().kthvalue(
+                          max(1, int(0.999 * int(both.sum())))).values), 8),
+                      "ao_occlusion_same_frac": round(occ_same, 6)},
+        "scene_bytes": {"instanced": int(inst_bytes), "flattened": int(flat_bytes)},
+        "instances": n_inst, "templates": len(templates), "flat_triangles": int(FI.shape[0]), "image": f"{w}x{h}",
+    }
+    line = _single_line(args, world, warmup, f"instanced city: {n_inst} instances of {len(templates)} 16-building "
+                        f"blocks ({FI.shape[0]/1e6:.2f}M tris flattened), {w}x{h} primary closest-hit + 1 AO any-hit "
+                        "ray per pixel; value = both instanced passes", world * 2 * n / (total_ms * 1e-3) / 1e6,
+                        total_ms, extra)
     if rank == 0:
         print(json.dumps(line), flush=True)
 

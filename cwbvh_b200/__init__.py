@@ -26,7 +26,7 @@ __all__ = [
     "autotune", "autotune_batch", "default_launch", "woopify", "gen_heightfield_boxes", "gen_city",
     "gen_spheres_terrain", "rtBindCWBVHData", "rtTraceCWBVH", "rtBindBVH2Data", "rtTraceBVH2",
     "rtOccludedCWBVH", "rtOccludedBVH2", "GenerateAORaysUniform", "version", "lib", "camera_rays",
-    "surfels_from_hits", "trace_ao", "load_mesh_dat", "save_mesh_dat", "load_samplecache_dat", "save_samplecache_dat",
+    "surfels_from_hits", "trace_ao", "Tlas", "trace_instanced", "build_tlas_host", "load_mesh_dat", "save_mesh_dat", "load_samplecache_dat", "save_samplecache_dat",
 ]
 
 
@@ -347,6 +347,74 @@ def trace_ordered(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stre
     """Trace in the oracle's traversal order (bit-identical results)."""
     check(lib.rq_trace_ordered(ctx._h, scene._h, _ptr(rays), _ptr(hits), _rows(rays, 8, "rays"), query,
                                _stream(stream)), "rq_trace_ordered")
+
+
+class Tlas:
+    """Instances of CWBVH scenes under a top-level CWBVH (rq_tlas_*).
+
+    transforms: (n, 3, 4) object-to-world affine matrices; blas_index: (n,)
+    indices into `blas`.  The bottom-level scenes are kept alive here."""
+
+    def __init__(self, blas: Sequence[Scene], transforms, blas_index):
+        m = np.ascontiguousarray(transforms, np.float32).reshape(-1, 12)
+        bi = np.ascontiguousarray(blas_index, np.int32).reshape(-1)
+        if m.shape[0] != bi.size:
+            raise ValueError("one transform per instance")
+        self._blas = list(blas)
+        arr = (C.c_void_p * len(self._blas))(*[b._h.value if isinstance(b._h, C.c_void_p) else b._h
+                                                for b in self._blas])
+        h = C.c_void_p()
+        check(lib.rq_tlas_create(arr, len(self._blas), m.ctypes.data, bi.ctypes.data, bi.size, C.byref(h)),
+              "rq_tlas_create")
+        self._h = h
+        self.n_instances = bi.size
+
+    def buffers(self) -> dict:
+        """Host copies of the top-level buffers (nodes, rows, map)."""
+        n, nn, r, nr, mp = C.c_void_p(), C.c_int64(), C.c_void_p(), C.c_int64(), C.c_void_p()
+        check(lib.rq_tlas_buffers(self._h, C.byref(n), C.byref(nn), C.byref(r), C.byref(nr), C.byref(mp)),
+              "rq_tlas_buffers")
+        f = lambda ptr, k, t: np.ctypeslib.as_array(C.cast(ptr, C.POINTER(t)), shape=(k,)).copy()  # noqa: E731
+        return {"nodes": f(n, 4 * nn.value, C.c_float).reshape(-1, 4),
+                "rows": f(r, 4 * nr.value, C.c_float).reshape(-1, 4),
+                "map": f(mp, nr.value, C.c_int32)}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_tlas_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def build_tlas_host(blas_bounds, transforms, blas_index) -> HostBVH:
+    """The top-level tree alone, built on the host (rq_tlas_build_host):
+    blas_bounds (n_blas, 6) lo/hi, transforms (n, 3, 4), blas_index (n,).
+    The result's nodes / woop / prim_index are the top-level nodes, the
+    instance rows and the (instance, blas, -1) map."""
+    bb = np.ascontiguousarray(blas_bounds, np.float32).reshape(-1, 6)
+    m = np.ascontiguousarray(transforms, np.float32).reshape(-1, 12)
+    bi = np.ascontiguousarray(blas_index, np.int32).reshape(-1)
+    if m.shape[0] != bi.size:
+        raise ValueError("one transform per instance")
+    h = C.c_void_p()
+    check(lib.rq_tlas_build_host(bb.ctypes.data, bb.shape[0], m.ctypes.data, bi.ctypes.data, bi.size, C.byref(h)),
+          "rq_tlas_build_host")
+    hb = HostBVH.__new__(HostBVH)
+    hb.vertices = hb.indices = None
+    hb._adopt(h)
+    hb.kind = CWBVH
+    return hb
+
+
+def trace_instanced(ctx: Context, tlas: Tlas, rays, hits, query: int = ANY, instance_out=None, stream=None) -> None:
+    """Trace world-space rays through a Tlas; instance_out (int32, one per
+    ray) receives the hit instance (-1 on a miss)."""
+    n = _rows(rays, 8, "rays")
+    check(lib.rq_trace_instanced(ctx._h, tlas._h, _ptr(rays), _ptr(hits),
+                                 _ptr(instance_out) if instance_out is not None else None, n, query,
+                                 _stream(stream)), "rq_trace_instanced")
 
 
 def trace_ao(ctx: Context, scene: Scene, rays, spp: int, occluded=None, launch: Optional[Launch] = None,

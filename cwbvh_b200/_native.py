@@ -154,3 +154,8 @@ _sig("rq_free_host", None, vp)
 _sig("rq_host_bvh_save", C.c_int, vp, cp)
 _sig("rq_host_bvh_load", C.c_int, cp, P(vp))
 _sig("rq_trace_ao", C.c_int, vp, vp, vp, i64, C.c_int, vp, P(Launch), vp)
+_sig("rq_tlas_create", C.c_int, P(vp), C.c_int, vp, vp, i64, P(vp))
+_sig("rq_tlas_destroy", C.c_int, vp)
+_sig("rq_tlas_buffers", C.c_int, vp, P(vp), P(i64), P(vp), P(i64), P(vp))
+_sig("rq_trace_instanced", C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, vp)
+_sig("rq_tlas_build_host", C.c_int, vp, C.c_int, vp, vp, i64, P(vp))

@@ -350,8 +350,8 @@ std::vector<PrimRef> make_refs(const Mesh& m, int max_frags) {
 
 }  // namespace
 
-void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
-                     Tree<2>& out, int max_frags) {
+static void build_from_refs(std::vector<PrimRef> refs, int max_leaf, int bins, int max_depth, bool big_leaves,
+                            int threads, Tree<2>& out) {
     Builder2 b;
     b.max_leaf = max_leaf;
     b.big_leaves = big_leaves;
@@ -359,7 +359,7 @@ void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool 
     b.max_depth = max_depth;
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     b.spare_threads = threads - 1;
-    b.refs = make_refs(m, max_frags);
+    b.refs = std::move(refs);
     const int64_t nt = (int64_t)b.refs.size();
     BBox all, call;
     for (const PrimRef& p : b.refs) {
@@ -392,6 +392,25 @@ void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool 
     b.leaves.resize(b.n_leaves.load());
     out.nodes = std::move(b.nodes);
     out.leaves = std::move(b.leaves);
+}
+
+void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
+                     Tree<2>& out, int max_frags) {
+    build_from_refs(make_refs(m, max_frags), max_leaf, bins, max_depth, big_leaves, threads, out);
+}
+
+void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_depth, int threads, Tree<2>& out) {
+    std::vector<PrimRef> refs((size_t)n);
+    for (int64_t k = 0; k < n; ++k) {
+        PrimRef& p = refs[(size_t)k];
+        for (int a = 0; a < 3; ++a) {
+            p.lo[a] = boxes[6 * k + a];
+            p.hi[a] = boxes[6 * k + 3 + a];
+        }
+        p.id = (int32_t)k;
+        p.pad = 0;
+    }
+    build_from_refs(std::move(refs), 1, bins, max_depth, false, threads, out);
 }
 
 // Optimal collapse of a binary tree into an 8-wide tree under a surface-area

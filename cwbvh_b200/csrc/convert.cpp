@@ -231,7 +231,24 @@ int8_t axis_exponent(float extent) {
 
 }  // namespace
 
+template <class EmitPrim>
+static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out);
+
 void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out) {
+    convert_cwbvh_impl(t, [&](int32_t prim) { append_triangle(m, prim, out); }, out);
+}
+
+void convert_cwbvh_instances(const Tree<8>& t, const float* rows12, const int32_t* extra, HostBVH& out) {
+    convert_cwbvh_impl(t, [&](int32_t k) {
+        out.woop.insert(out.woop.end(), rows12 + 12 * (int64_t)k, rows12 + 12 * (int64_t)k + 12);
+        out.prim_index.push_back(k);
+        out.prim_index.push_back(extra[k]);
+        out.prim_index.push_back(-1);
+    }, out);
+}
+
+template <class EmitPrim>
+static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out) {
     out.kind = RQ_BVH_CWBVH;
     out.nodes.assign(20, 0.0f);  // root slot
     out.woop.clear();
@@ -306,7 +323,7 @@ void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out) {
                 const uint32_t unary = lf.count == 1 ? 1u : (lf.count == 2 ? 3u : 7u);
                 meta = (uint8_t)((unary << 5) | ((uint32_t)leaf_tris & 31u));
                 leaf_tris += lf.count;
-                for (int32_t k = 0; k < lf.count; ++k) append_triangle(m, t.prim_refs[lf.first + k], out);
+                for (int32_t k = 0; k < lf.count; ++k) emit(t.prim_refs[lf.first + k]);
                 ++n_leaves;
             }
             node_bytes = reinterpret_cast<uint8_t*>(&out.nodes[(size_t)it.addr * 4]);

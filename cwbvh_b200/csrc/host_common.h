@@ -110,6 +110,9 @@ struct HostBVH {
 // references with clipped bounds (power of two).
 void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
                      Tree<2>& out, int max_frags = 1);
+// Binary tree over axis-aligned boxes (lo xyz, hi xyz per box; box k is
+// primitive k), e.g. the world bounds of instances for a top-level tree.
+void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_depth, int threads, Tree<2>& out);
 void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out);
 int tree_depth2(const Tree<2>& t);
 int tree_depth8(const Tree<8>& t);
@@ -118,6 +121,10 @@ int tree_depth8(const Tree<8>& t);
 void woopify(const V3& v0, const V3& v1, const V3& v2, float out[12]);
 void convert_bvh2(const Tree<2>& t, const Mesh& m, HostBVH& out);
 void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out);
+// CWBVH nodes over a tree of instances: each leaf primitive k is emitted as
+// the 3 rows of rows12[12 k ..] (the instance's world-to-object transform) in
+// place of Woop rows, with primitive-map entries (k, extra[k], -1).
+void convert_cwbvh_instances(const Tree<8>& t, const float* rows12, const int32_t* extra, HostBVH& out);
 
 // Scene generators (scenegen.cpp)
 void gen_heightfield_boxes(uint64_t seed, int grid, int n_boxes, float bmin, float bmax, Mesh& m);

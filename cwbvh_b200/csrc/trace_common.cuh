@@ -84,4 +84,45 @@ __device__ __forceinline__ float byte_to_float(unsigned word, unsigned byte_inde
     return __fsub_rn(__uint_as_float(r), 8388608.0f);
 }
 
+// Hit mask of the 8 children of one CWBVH node (src/TraversalKernelCWBVH.cu:
+// 141-288): bits 24-31 for inner children at 24 + (slot ^ octinv), the
+// unary triangle counts at their offsets for leaf children.  The slab
+// extremes are taken as the reference does, on the float bits compared as
+// signed integers, then clamped by tmin / tmax with float min/max.
+__device__ __forceinline__ unsigned cwbvh_hitmask(const float4& n1, const float4& n2, const float4& n3,
+                                                  const float4& n4, float adjx, float adjy, float adjz, float orx,
+                                                  float ory, float orz, bool negx, bool negy, bool negz,
+                                                  unsigned octinv4, float tmin, float tmax) {
+    unsigned hitmask = 0u;
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+        const unsigned meta4 = __float_as_uint(g == 0 ? n1.z : n1.w);
+        const unsigned inner4 = ((meta4 & (meta4 << 1)) & 0x10101010u) >> 4;
+        const unsigned bitidx4 = (meta4 ^ (octinv4 & (inner4 * 0xFFu))) & 0x1F1F1F1Fu;
+        const unsigned bits4 = (meta4 >> 5) & 0x07070707u;
+        const unsigned wlx = __float_as_uint(g == 0 ? n2.x : n2.y);
+        const unsigned whx = __float_as_uint(g == 0 ? n3.z : n3.w);
+        const unsigned wly = __float_as_uint(g == 0 ? n2.z : n2.w);
+        const unsigned why = __float_as_uint(g == 0 ? n4.x : n4.y);
+        const unsigned wlz = __float_as_uint(g == 0 ? n3.x : n3.y);
+        const unsigned whz = __float_as_uint(g == 0 ? n4.z : n4.w);
+        const unsigned lox = negx ? whx : wlx, hix = negx ? wlx : whx;
+        const unsigned loy = negy ? why : wly, hiy = negy ? wly : why;
+        const unsigned loz = negz ? whz : wlz, hiz = negz ? wlz : whz;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float tx0 = __fmaf_rn(byte_to_float(lox, c), adjx, orx);
+            const float ty0 = __fmaf_rn(byte_to_float(loy, c), adjy, ory);
+            const float tz0 = __fmaf_rn(byte_to_float(loz, c), adjz, orz);
+            const float tx1 = __fmaf_rn(byte_to_float(hix, c), adjx, orx);
+            const float ty1 = __fmaf_rn(byte_to_float(hiy, c), adjy, ory);
+            const float tz1 = __fmaf_rn(byte_to_float(hiz, c), adjz, orz);
+            const float cmin = fmaxf(imax3(tx0, ty0, tz0), tmin);
+            const float cmax = fminf(imin3(tx1, ty1, tz1), tmax);
+            if (cmin <= cmax) hitmask |= ((bits4 >> (8 * c)) & 0xFFu) << ((bitidx4 >> (8 * c)) & 0xFFu);
+        }
+    }
+    return hitmask;
+}
+
 }  // namespace rq

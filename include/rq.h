@@ -447,6 +447,38 @@ rq_status rq_rtOccludedBVH2(void* rays, void* hits, int ray_count);
 rq_status rq_device_copy(void* dst, const void* src, int64_t bytes);
 rq_status rq_device_free(void* p);
 
+/* ------------------------------------------------------- instancing (TLAS) */
+/*
+ * Two-level scenes (no reference counterpart: the reference traces one flat
+ * scene).  A top-level CWBVH is built over instances of bottom-level CWBVH
+ * scenes; instance k places scene blas[blas_index[k]] with the affine
+ * object-to-world transform object_to_world[12 k .. 12 k + 11] (3 x 4,
+ * row-major: world = M [p; 1]).  Rays are traced in world space; each hit
+ * reports t (the same in world and object space), the Woop address within
+ * its bottom-level scene, u, v, and -- in instance_out, if not NULL -- the
+ * instance (-1 on a miss).  The bottom-level scenes are borrowed: keep them
+ * alive while the top level is in use.  Singular or non-finite transforms,
+ * BVH2 scenes and out-of-range indices give RQ_ERR_INVALID_ARG.
+ */
+typedef struct rq_tlas* rq_tlas_t;
+rq_status rq_tlas_create(const rq_scene_t* blas, int n_blas, const float* object_to_world,
+                         const int32_t* blas_index, int64_t n_instances, rq_tlas_t* out);
+rq_status rq_tlas_destroy(rq_tlas_t tlas);
+/* The top-level tree alone, built on the host from the bottom-level scenes'
+ * bounds (6 floats each: lo xyz, hi xyz): nodes, instance rows in place of
+ * Woop rows and the (instance, bottom-level index, -1) map, as a host BVH
+ * handle (rq_host_bvh_buffers / rq_host_bvh_free).  rq_tlas_create runs this
+ * with the scenes' bounds and uploads the result. */
+rq_status rq_tlas_build_host(const float* blas_bounds, int n_blas, const float* object_to_world,
+                             const int32_t* blas_index, int64_t n_instances, rq_host_bvh_t* out);
+/* Host copies of the top-level buffers: nodes, instance rows (the
+ * world-to-object transform, 3 float4 per instance slot) and the map
+ * (instance, bottom-level index, -1) per row. */
+rq_status rq_tlas_buffers(rq_tlas_t tlas, const float** nodes, int64_t* node_float4s,
+                          const float** rows, int64_t* row_float4s, const int32_t** map);
+rq_status rq_trace_instanced(rq_ctx_t ctx, rq_tlas_t tlas, const rq_ray* rays, rq_hit* hits,
+                             int32_t* instance_out, int64_t count, rq_query query, void* stream);
+
 /* ------------------------------------------------------------- device info */
 int rq_device_sm_count(void);
 /* L2 read-bandwidth probe (a measurement utility; no reference counterpart):

@@ -72,6 +72,47 @@ static inline int woop_test(const f4* v, const float o[3], const float d[3], flo
 
 #define STACK_CAP 256
 
+/* Node test of one CWBVH node (src/TraversalKernelCWBVH.cu:117-289): the next
+ * node group (child base, inner hit bits | imask) and triangle group. */
+static void cwbvh_visit(const f4* n, const float o[3], const float idir[3], uint32_t octinv, float tmin, float tmax,
+                        uint32_t* ngx_, uint32_t* ngy_, uint32_t* tgx_, uint32_t* tgy_) {
+    const uint32_t ew = ubits(n[0].w);
+    float adj[3], org[3];
+    for (int a = 0; a < 3; ++a) {
+        const int e = (int)(int8_t)((ew >> (8 * a)) & 0xFFu);
+        adj[a] = from_u(((uint32_t)(e + 127)) << 23) * idir[a];
+    }
+    org[0] = -(o[0] - n[0].x) * idir[0];
+    org[1] = -(o[1] - n[0].y) * idir[1];
+    org[2] = -(o[2] - n[0].z) * idir[2];
+    uint32_t hitmask = 0;
+    for (int c = 0; c < 8; ++c) {
+        const int g = c >> 2, k = c & 3;
+        const uint32_t meta = (ubits(g ? n[1].w : n[1].z) >> (8 * k)) & 0xFFu;
+        const int inner = (meta & 0x18u) == 0x18u;
+        const uint32_t bitidx = (inner ? (meta ^ octinv) : meta) & 0x1Fu;
+        const uint32_t cbits = (meta >> 5) & 7u;
+        /* qlo/qhi words: x lo n2.x|n2.y, x hi n3.z|n3.w, y lo n2.z|n2.w,
+         * y hi n4.x|n4.y, z lo n3.x|n3.y, z hi n4.z|n4.w */
+        const uint32_t wl[3] = {ubits(g ? n[2].y : n[2].x), ubits(g ? n[2].w : n[2].z), ubits(g ? n[3].y : n[3].x)};
+        const uint32_t wh[3] = {ubits(g ? n[3].w : n[3].z), ubits(g ? n[4].y : n[4].x), ubits(g ? n[4].w : n[4].z)};
+        float t0[3], t1[3];
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t lo = idir[a] < 0.f ? wh[a] : wl[a];
+            const uint32_t hi = idir[a] < 0.f ? wl[a] : wh[a];
+            t0[a] = fmaf((float)((lo >> (8 * k)) & 0xFFu), adj[a], org[a]);
+            t1[a] = fmaf((float)((hi >> (8 * k)) & 0xFFu), adj[a], org[a]);
+        }
+        const float cmin = fmaxf(imax3f(t0[0], t0[1], t0[2]), tmin);
+        const float cmax = fminf(imin3f(t1[0], t1[1], t1[2]), tmax);
+        if (cmin <= cmax) hitmask |= cbits << bitidx;
+    }
+    *ngx_ = ubits(n[1].x);
+    *ngy_ = (hitmask & 0xFF000000u) | (ew >> 24);
+    *tgx_ = ubits(n[1].y);
+    *tgy_ = hitmask & 0x00FFFFFFu;
+}
+
 /* One ray through the CWBVH (src/TraversalKernelCWBVH.cu:74-363). */
 static int cwbvh_ray(const f4* nodes, int64_t node_f4, const f4* woop, int64_t woop_f4, const float* ray, int any,
                      float* hit, int32_t* nvis, int32_t* ntri) {
@@ -101,41 +142,7 @@ static int cwbvh_ray(const f4* nodes, int64_t node_f4, const f4* woop, int64_t w
             if ((uint64_t)ci * 5u + 5u > (uint64_t)node_f4) { err |= ORACLE_ERR_BAD_SCENE; break; }
             const f4* n = nodes + (size_t)ci * 5u;
             ++visits;
-            const uint32_t ew = ubits(n[0].w);
-            float adj[3], org[3];
-            for (int a = 0; a < 3; ++a) {
-                const int e = (int)(int8_t)((ew >> (8 * a)) & 0xFFu);
-                adj[a] = from_u(((uint32_t)(e + 127)) << 23) * idir[a];
-            }
-            org[0] = -(o[0] - n[0].x) * idir[0];
-            org[1] = -(o[1] - n[0].y) * idir[1];
-            org[2] = -(o[2] - n[0].z) * idir[2];
-            uint32_t hitmask = 0;
-            for (int c = 0; c < 8; ++c) {
-                const int g = c >> 2, k = c & 3;
-                const uint32_t meta = (ubits(g ? n[1].w : n[1].z) >> (8 * k)) & 0xFFu;
-                const int inner = (meta & 0x18u) == 0x18u;
-                const uint32_t bitidx = (inner ? (meta ^ octinv) : meta) & 0x1Fu;
-                const uint32_t cbits = (meta >> 5) & 7u;
-                /* qlo/qhi words: x lo n2.x|n2.y, x hi n3.z|n3.w, y lo n2.z|n2.w,
-                 * y hi n4.x|n4.y, z lo n3.x|n3.y, z hi n4.z|n4.w */
-                const uint32_t wl[3] = {ubits(g ? n[2].y : n[2].x), ubits(g ? n[2].w : n[2].z), ubits(g ? n[3].y : n[3].x)};
-                const uint32_t wh[3] = {ubits(g ? n[3].w : n[3].z), ubits(g ? n[4].y : n[4].x), ubits(g ? n[4].w : n[4].z)};
-                float t0[3], t1[3];
-                for (int a = 0; a < 3; ++a) {
-                    const uint32_t lo = idir[a] < 0.f ? wh[a] : wl[a];
-                    const uint32_t hi = idir[a] < 0.f ? wl[a] : wh[a];
-                    t0[a] = fmaf((float)((lo >> (8 * k)) & 0xFFu), adj[a], org[a]);
-                    t1[a] = fmaf((float)((hi >> (8 * k)) & 0xFFu), adj[a], org[a]);
-                }
-                const float cmin = fmaxf(imax3f(t0[0], t0[1], t0[2]), tmin);
-                const float cmax = fminf(imin3f(t1[0], t1[1], t1[2]), tmax);
-                if (cmin <= cmax) hitmask |= cbits << bitidx;
-            }
-            ngx = ubits(n[1].x);
-            ngy = (hitmask & 0xFF000000u) | (ew >> 24);
-            tgx = ubits(n[1].y);
-            tgy = hitmask & 0x00FFFFFFu;
+            cwbvh_visit(n, o, idir, octinv, tmin, tmax, &ngx, &ngy, &tgx, &tgy);
         } else {
             tgx = ngx; tgy = ngy;
             ngx = 0; ngy = 0;
@@ -257,6 +264,127 @@ int oracle_trace(int kind, const float* nodes, int64_t node_f4, const float* woo
         else
             err |= bvh2_ray((const f4*)nodes, node_f4, (const f4*)woop, woop_f4, rays + 8 * i, any_hit, hits + 4 * i, nv, nt);
     }
+    (void)threads;
+    return err;
+}
+
+/* One ray through a two-level scene: a top-level CWBVH whose leaf "triangles"
+ * are instances (3 rows of the world-to-object transform where the Woop rows
+ * would be; map entries (instance, bottom-level index, -1)) over bottom-level
+ * CWBVHs.  This is the library's own extension (the reference has no
+ * instancing); the traversal order -- push the top level's node group, then
+ * its instance group, enter the instance, leave it when its stack part is
+ * empty -- is the one the GPU kernel follows. */
+static int inst_ray(const f4* tn, int64_t tn_f4, const f4* rows, int64_t rows_f4, const int32_t* map, int n_blas,
+                    const float* const* bn, const int64_t* bn_f4, const float* const* bw, const int64_t* bw_f4,
+                    const float* ray, int any, float* hit, int32_t* inst_out) {
+    const float wo[3] = {ray[0], ray[1], ray[2]}, wd[3] = {ray[4], ray[5], ray[6]};
+    const float tmin = ray[3];
+    float tmax = ray[7];
+    float o[3], d[3], idir[3];
+    uint32_t octinv;
+    const f4* nodes = tn;
+    const f4* woop = rows;
+    int64_t node_f4 = tn_f4, woop_f4 = rows_f4;
+    int in_blas = 0, inst_sp = 0, cur_inst = -1, hit_inst = -1;
+#define SET_RAY(O, D)                                                                                         \
+    do {                                                                                                      \
+        for (int a_ = 0; a_ < 3; ++a_) { o[a_] = (O)[a_]; d[a_] = (D)[a_]; idir[a_] = guarded_rcp(d[a_]); } \
+        octinv = 7u - (((d[0] < 0.f) ? 4u : 0u) | ((d[1] < 0.f) ? 2u : 0u) | ((d[2] < 0.f) ? 1u : 0u));     \
+    } while (0)
+    SET_RAY(wo, wd);
+    uint32_t ngx = 0, ngy = 0x80000000u, tgx = 0, tgy = 0;
+    uint32_t stx[STACK_CAP], sty[STACK_CAP];
+    int sp = 0, hit_addr = -1, err = 0;
+    float hu = 0.f, hv = 0.f;
+
+    for (;;) {
+        if (ngy > 0x00FFFFFFu) {
+            const uint32_t hits = ngy;
+            const unsigned bit = bfind(hits);
+            const uint32_t base = ngx;
+            ngy &= ~(1u << bit);
+            if (ngy > 0x00FFFFFFu) {
+                if (sp >= STACK_CAP) { err |= ORACLE_ERR_STACK; break; }
+                stx[sp] = ngx; sty[sp] = ngy; ++sp;
+            }
+            const unsigned slot = (bit - 24u) ^ octinv;
+            const uint32_t ci = base + (uint32_t)__builtin_popcount(hits & ~(0xFFFFFFFFu << slot));
+            if ((uint64_t)ci * 5u + 5u > (uint64_t)node_f4) { err |= ORACLE_ERR_BAD_SCENE; break; }
+            cwbvh_visit(nodes + (size_t)ci * 5u, o, idir, octinv, tmin, tmax, &ngx, &ngy, &tgx, &tgy);
+        } else {
+            tgx = ngx; tgy = ngy;
+            ngx = 0; ngy = 0;
+        }
+        int done = 0;
+        while (tgy != 0) {
+            const unsigned ti = bfind(tgy);
+            const uint32_t tri = tgx * 3u + ti * 3u;
+            tgy &= ~(1u << ti);
+            if ((uint64_t)tri + 3u > (uint64_t)woop_f4) { err |= ORACLE_ERR_BAD_SCENE; done = 1; break; }
+            if (in_blas) {
+                float t, u, v;
+                if (woop_test(woop + tri, o, d, tmin, tmax, &t, &u, &v)) {
+                    tmax = t; hit_addr = (int)tri; hit_inst = cur_inst; hu = u; hv = v;
+                    if (any) { done = 1; break; }
+                }
+            } else {
+                const int32_t inst = map[tri], b = map[tri + 1];
+                if (b < 0 || b >= n_blas) { err |= ORACLE_ERR_BAD_SCENE; done = 1; break; }
+                if (ngy > 0x00FFFFFFu) {
+                    if (sp >= STACK_CAP) { err |= ORACLE_ERR_STACK; done = 1; break; }
+                    stx[sp] = ngx; sty[sp] = ngy; ++sp;
+                }
+                if (tgy != 0) {
+                    if (sp >= STACK_CAP) { err |= ORACLE_ERR_STACK; done = 1; break; }
+                    stx[sp] = tgx; sty[sp] = tgy; ++sp;
+                }
+                inst_sp = sp; in_blas = 1; cur_inst = inst;
+                const f4* r = woop + tri;
+                const float oo[3] = {fmaf(r[0].z, wo[2], fmaf(r[0].y, wo[1], fmaf(r[0].x, wo[0], r[0].w))),
+                                     fmaf(r[1].z, wo[2], fmaf(r[1].y, wo[1], fmaf(r[1].x, wo[0], r[1].w))),
+                                     fmaf(r[2].z, wo[2], fmaf(r[2].y, wo[1], fmaf(r[2].x, wo[0], r[2].w)))};
+                const float od[3] = {fmaf(r[0].z, wd[2], fmaf(r[0].y, wd[1], r[0].x * wd[0])),
+                                     fmaf(r[1].z, wd[2], fmaf(r[1].y, wd[1], r[1].x * wd[0])),
+                                     fmaf(r[2].z, wd[2], fmaf(r[2].y, wd[1], r[2].x * wd[0]))};
+                SET_RAY(oo, od);
+                nodes = (const f4*)bn[b]; node_f4 = bn_f4[b];
+                woop = (const f4*)bw[b]; woop_f4 = bw_f4[b];
+                ngx = 0; ngy = 0x80000000u; tgx = 0; tgy = 0;
+                break;
+            }
+        }
+        if (done) break;
+        if (ngy <= 0x00FFFFFFu) {
+            if (in_blas && sp == inst_sp) {
+                in_blas = 0;
+                nodes = tn; node_f4 = tn_f4; woop = rows; woop_f4 = rows_f4;
+                SET_RAY(wo, wd);
+            }
+            if (sp > 0) { --sp; ngx = stx[sp]; ngy = sty[sp]; }
+            else break;
+        }
+    }
+#undef SET_RAY
+    if (err) { hit_addr = -1; hit_inst = -1; }
+    hit[0] = tmax; hit[1] = from_i(hit_addr); hit[2] = hu; hit[3] = hv;
+    if (inst_out) *inst_out = hit_addr >= 0 ? hit_inst : -1;
+    return err;
+}
+
+int oracle_trace_instanced(const float* tlas_nodes, int64_t tlas_node_f4, const float* tlas_rows, int64_t tlas_rows_f4,
+                           const int32_t* tlas_map, int n_blas, const float* const* blas_nodes,
+                           const int64_t* blas_node_f4, const float* const* blas_woop, const int64_t* blas_woop_f4,
+                           const float* rays, int64_t n, int any_hit, float* hits, int32_t* inst_out, int threads) {
+    int err = 0;
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) reduction(| : err) num_threads(threads)
+#endif
+    for (int64_t i = 0; i < n; ++i)
+        err |= inst_ray((const f4*)tlas_nodes, tlas_node_f4, (const f4*)tlas_rows, tlas_rows_f4, tlas_map, n_blas,
+                        blas_nodes, blas_node_f4, blas_woop, blas_woop_f4, rays + 8 * i, any_hit, hits + 4 * i,
+                        inst_out ? inst_out + i : NULL);
     (void)threads;
     return err;
 }

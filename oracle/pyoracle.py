@@ -35,6 +35,9 @@ def oracle():
         lib.oracle_philox.restype = None
         lib.oracle_philox.argtypes = [vp, C.c_uint32, C.c_uint32, vp]
         lib.oracle_max_threads.restype = C.c_int
+        lib.oracle_trace_instanced.restype = C.c_int
+        lib.oracle_trace_instanced.argtypes = [vp, i64, vp, i64, vp, C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, vp,
+                                               vp, C.c_int]
         _oracle = lib
     return _oracle
 
@@ -88,6 +91,31 @@ def trace(kind: int, nodes: np.ndarray, woop: np.ndarray, rays: np.ndarray, any_
     if err:
         raise RuntimeError(f"oracle traversal error bits {err}")
     return (hits, nv, nt) if counts else hits
+
+
+def trace_instanced(tlas: dict, blas: list, rays: np.ndarray, any_hit: bool, threads: int = 0):
+    """CPU two-level traversal.  tlas: {"nodes", "rows", "map"} host arrays
+    (the library's top-level buffers); blas: [(nodes, woop), ...] of the
+    bottom-level CWBVHs.  Returns (hits (n, 4) float32, instance (n,) int32)."""
+    tn = np.ascontiguousarray(tlas["nodes"], np.float32)
+    tr = np.ascontiguousarray(tlas["rows"], np.float32)
+    tm = np.ascontiguousarray(tlas["map"], np.int32)
+    bn = [np.ascontiguousarray(n, np.float32) for n, _ in blas]
+    bw = [np.ascontiguousarray(w, np.float32) for _, w in blas]
+    nb = len(blas)
+    bn_p = (C.c_void_p * nb)(*[_p(a) for a in bn])
+    bw_p = (C.c_void_p * nb)(*[_p(a) for a in bw])
+    bn_n = np.array([a.size // 4 for a in bn], np.int64)
+    bw_n = np.array([a.size // 4 for a in bw], np.int64)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = rays.shape[0]
+    hits = np.zeros((n, 4), np.float32)
+    inst = np.zeros(n, np.int32)
+    err = oracle().oracle_trace_instanced(_p(tn), tn.size // 4, _p(tr), tr.size // 4, _p(tm), nb, bn_p, _p(bn_n),
+                                          bw_p, _p(bw_n), _p(rays), n, int(any_hit), _p(hits), _p(inst), threads)
+    if err:
+        raise RuntimeError(f"oracle traversal error bits {err}")
+    return hits, inst
 
 
 def tri_f64(ray: np.ndarray, v0, v1, v2) -> np.ndarray:
