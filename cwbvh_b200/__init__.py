@@ -408,13 +408,18 @@ def build_tlas_host(blas_bounds, transforms, blas_index) -> HostBVH:
     return hb
 
 
-def trace_instanced(ctx: Context, tlas: Tlas, rays, hits, query: int = ANY, instance_out=None, stream=None) -> None:
+def trace_instanced(ctx: Context, tlas: Tlas, rays, hits, query: int = ANY, instance_out=None,
+                    launch: Optional[Launch] = None, stream=None, ordered: bool = False) -> None:
     """Trace world-space rays through a Tlas; instance_out (int32, one per
-    ray) receives the hit instance (-1 on a miss)."""
+    ray) receives the hit instance (-1 on a miss).  ordered=True turns
+    postponing off: the oracle's traversal order, bit-identical results."""
     n = _rows(rays, 8, "rays")
+    if ordered:
+        launch = Launch(0, 0, 0, -1.0, 0, 0)
     check(lib.rq_trace_instanced(ctx._h, tlas._h, _ptr(rays), _ptr(hits),
                                  _ptr(instance_out) if instance_out is not None else None, n, query,
-                                 _stream(stream)), "rq_trace_instanced")
+                                 C.byref(launch) if launch is not None else None, _stream(stream)),
+          "rq_trace_instanced")
 
 
 def trace_ao(ctx: Context, scene: Scene, rays, spp: int, occluded=None, launch: Optional[Launch] = None,

@@ -157,5 +157,5 @@ _sig("rq_trace_ao", C.c_int, vp, vp, vp, i64, C.c_int, vp, P(Launch), vp)
 _sig("rq_tlas_create", C.c_int, P(vp), C.c_int, vp, vp, i64, P(vp))
 _sig("rq_tlas_destroy", C.c_int, vp)
 _sig("rq_tlas_buffers", C.c_int, vp, P(vp), P(i64), P(vp), P(i64), P(vp))
-_sig("rq_trace_instanced", C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, vp)
+_sig("rq_trace_instanced", C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, P(Launch), vp)
 _sig("rq_tlas_build_host", C.c_int, vp, C.c_int, vp, vp, i64, P(vp))

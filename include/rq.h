@@ -476,8 +476,12 @@ rq_status rq_tlas_build_host(const float* blas_bounds, int n_blas, const float* 
  * (instance, bottom-level index, -1) per row. */
 rq_status rq_tlas_buffers(rq_tlas_t tlas, const float** nodes, int64_t* node_float4s,
                           const float** rows, int64_t* row_float4s, const int32_t** map);
+/* launch: NULL for the defaults; only postpone_ratio (triangle / instance
+ * postponing as in rq_trace, but off unless a positive ratio is given: off is
+ * the oracle's traversal order) and fetch_nd / fetch_nw are used. */
 rq_status rq_trace_instanced(rq_ctx_t ctx, rq_tlas_t tlas, const rq_ray* rays, rq_hit* hits,
-                             int32_t* instance_out, int64_t count, rq_query query, void* stream);
+                             int32_t* instance_out, int64_t count, rq_query query,
+                             const rq_launch* launch, void* stream);
 
 /* ------------------------------------------------------------- device info */
 int rq_device_sm_count(void);
