@@ -251,7 +251,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving configuration")
     ap.add_argument("--profile", action="store_true",
-                    help="batched/small: build the workload and only run the batch W+K times (profiler captures)")
+                    help="batched/small/large: build the workload and only run the trace W+K times (profiler captures)")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -1002,6 +1002,13 @@ def run_large(args, world, rank, dist):
         n = rays.shape[0]
         hits = torch.empty((n, 4), device="cuda")
         shits = torch.empty((n, 4), device="cuda")
+    if args.profile:  # profiler captures: only the unsorted trace, W + K launches
+        for _ in range(warmup + args.steps):
+            rq.trace(ctx, sc, rays, hits, rq.ANY, stream=stream)
+        torch.cuda.synchronize()
+        ctx.check(stream)
+        log(f"[bench] profile mode: {warmup + args.steps} traces of {n} rays")
+        return
     ms_plain = time_steps(lambda: rq.trace(ctx, sc, rays, hits, rq.ANY, stream=stream), args.steps, warmup, stream,
                           dist)
     with torch.cuda.stream(stream):
@@ -1023,8 +1030,9 @@ def run_large(args, world, rank, dist):
     occ = float((hits[:, 1].view(torch.int32) != -1).float().mean().item())
     fused_same = bool(torch.equal(occl, (hits[:, 1].view(torch.int32) != -1).view(-1, spp).sum(1, dtype=torch.int32)))
     peak, peak_kind = measured_peak_hbm()
+    l2 = measure_l2_read(stream)
     alg = _counted_bytes(ctx, sc, rays, rq.ANY, stream)
-    unsorted = _pass("unsorted", n, ms_plain, alg, peak)
+    unsorted = _pass("unsorted", n, ms_plain, alg, peak, l2)
     best = min(ms_plain, ms_sorted, ms_fused)
     extra = {
         "passes": {"unsorted": unsorted,
@@ -1037,7 +1045,10 @@ def run_large(args, world, rank, dist):
         "ao_occluded_fraction": round(occ, 4),
         "triangles": int(I.shape[0]), "scene_bytes": int(hb.nodes.nbytes + hb.woop.nbytes),
         "roofline": {"bound": "hbm", "achieved": unsorted["achieved_gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": unsorted["hbm_frac"], "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                     "frac": unsorted["hbm_frac"], "peak_source": f"hbm_gbs of {peak_kind}",
+                     "traffic": (profile_traffic("large" + ("_quick" if args.quick else "")) or {}).get(
+                         "dram_bytes_per_launch"),
+                     "l2": {"peak": round(l2, 1), "frac": unsorted["l2_frac"]},
                      "kernel": "unsorted AO any-hit trace"},
     }
     line = _single_line(args, world, warmup, f"large: {I.shape[0]/1e6:.1f}M tris, {n_surf} surfels x {spp} spp "
