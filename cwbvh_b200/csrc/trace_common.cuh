@@ -13,7 +13,6 @@
 // reproducible on the CPU and at least as accurate.
 #pragma once
 
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -85,20 +84,6 @@ __device__ __forceinline__ float byte_to_float(unsigned word, unsigned byte_inde
     return __fsub_rn(__uint_as_float(r), 8388608.0f);
 }
 
-#ifndef RQ_HALF_BYTES
-#define RQ_HALF_BYTES 0
-#endif
-
-// Bytes c and c+1 (c even) of `word` as two subnormal halves, b * 2^-24
-// (one PRMT); each widens exactly to float.
-__device__ __forceinline__ __half2 byte_pair(unsigned word, unsigned c) {
-    unsigned r;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(word), "r"(0u), "r"(c == 0 ? 0x4140u : 0x4342u));
-    __half2 h;
-    memcpy(&h, &r, sizeof(h));
-    return h;
-}
-
 // Hit mask of the 8 children of one CWBVH node (src/TraversalKernelCWBVH.cu:
 // 141-288): bits 24-31 for inner children at 24 + (slot ^ octinv), the
 // unary triangle counts at their offsets for leaf children.  The slab
@@ -124,36 +109,6 @@ __device__ __forceinline__ unsigned cwbvh_hitmask(const float4& n1, const float4
         const unsigned lox = negx ? whx : wlx, hix = negx ? wlx : whx;
         const unsigned loy = negy ? why : wly, hiy = negy ? wly : why;
         const unsigned loz = negz ? whz : wlz, hiz = negz ? wlz : whz;
-#if RQ_HALF_BYTES
-        // Bytes c and c+1 of a plane word as two subnormal halves (b * 2^-24,
-        // one PRMT), widened exactly to floats; the slopes carry the 2^24 back
-        // (exact: a power-of-two scale), so fma(b 2^-24, adj 2^24, or) rounds
-        // the same real number as fma(b, adj, or).
-        const float ax = __fmul_rn(adjx, 16777216.0f), ay = __fmul_rn(adjy, 16777216.0f);
-        const float az = __fmul_rn(adjz, 16777216.0f);
-#pragma unroll
-        for (int c = 0; c < 4; c += 2) {
-            const __half2 lx = byte_pair(lox, c), ly = byte_pair(loy, c), lz = byte_pair(loz, c);
-            const __half2 hx = byte_pair(hix, c), hy = byte_pair(hiy, c), hz = byte_pair(hiz, c);
-            {
-                const float cmin = fmaxf(imax3(__fmaf_rn(__low2float(lx), ax, orx), __fmaf_rn(__low2float(ly), ay, ory),
-                                               __fmaf_rn(__low2float(lz), az, orz)), tmin);
-                const float cmax = fminf(imin3(__fmaf_rn(__low2float(hx), ax, orx), __fmaf_rn(__low2float(hy), ay, ory),
-                                               __fmaf_rn(__low2float(hz), az, orz)), tmax);
-                if (cmin <= cmax) hitmask |= ((bits4 >> (8 * c)) & 0xFFu) << ((bitidx4 >> (8 * c)) & 0xFFu);
-            }
-            {
-                const float cmin = fmaxf(imax3(__fmaf_rn(__high2float(lx), ax, orx),
-                                               __fmaf_rn(__high2float(ly), ay, ory),
-                                               __fmaf_rn(__high2float(lz), az, orz)), tmin);
-                const float cmax = fminf(imin3(__fmaf_rn(__high2float(hx), ax, orx),
-                                               __fmaf_rn(__high2float(hy), ay, ory),
-                                               __fmaf_rn(__high2float(hz), az, orz)), tmax);
-                if (cmin <= cmax)
-                    hitmask |= ((bits4 >> (8 * c + 8)) & 0xFFu) << ((bitidx4 >> (8 * c + 8)) & 0xFFu);
-            }
-        }
-#else
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const float tx0 = __fmaf_rn(byte_to_float(lox, c), adjx, orx);
@@ -166,7 +121,6 @@ __device__ __forceinline__ unsigned cwbvh_hitmask(const float4& n1, const float4
             const float cmax = fminf(imin3(tx1, ty1, tz1), tmax);
             if (cmin <= cmax) hitmask |= ((bits4 >> (8 * c)) & 0xFFu) << ((bitidx4 >> (8 * c)) & 0xFFu);
         }
-#endif
     }
     return hitmask;
 }
