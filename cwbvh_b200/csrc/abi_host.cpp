@@ -2,6 +2,8 @@
 // transform, procedural scenes and status strings.  Nothing here touches the
 // GPU, so these calls work on a machine without one.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <new>
 
@@ -78,10 +80,19 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
             h->b.depth = tree_depth2(h->b.tree2);
         } else {
             // The 8-wide tree's leaves hold at most 3 triangles (3 meta bits).
+            const auto t0 = std::chrono::steady_clock::now();
             build_bvh2_tree(m, 3, bp.sah_bins, 48, false, bp.threads, h->b.tree2, bp.presplit);
-            collapse_to_bvh8(h->b.tree2, h->b.tree8);
-            convert_cwbvh(h->b.tree8, m, h->b);
+            const auto t1 = std::chrono::steady_clock::now();
+            collapse_to_bvh8(h->b.tree2, h->b.tree8, bp.threads);
+            const auto t2 = std::chrono::steady_clock::now();
+            convert_cwbvh(h->b.tree8, m, h->b, bp.threads);
+            const auto t3 = std::chrono::steady_clock::now();
             h->b.depth = tree_depth8(h->b.tree8);
+            if (std::getenv("RQ_LOG")) {
+                auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+                std::fprintf(stderr, "rq_build_bvh: %lld tris, binary SAH %.1f ms, 8-wide collapse %.1f ms, "
+                             "CWBVH conversion %.1f ms\n", (long long)nt, ms(t0, t1), ms(t1, t2), ms(t2, t3));
+            }
         }
     } catch (const std::bad_alloc&) {
         delete h;

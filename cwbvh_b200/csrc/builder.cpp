@@ -455,16 +455,9 @@ struct Collapse {
         return kLeafCost * a * (float)t.leaves[-code - 2].count;  // a binary leaf stays one leaf
     }
 
-    void run() {
-        const size_t n = t.nodes.size();
-        best.assign(n * 9, INFINITY);
-        how.assign(n * 9, 0);
-        node_split.assign(n, 4);
-        prims.assign(n, 0);
-        // Post-order (parallel builds interleave node numbering).
-        std::vector<int32_t> order;
-        order.reserve(n);
-        std::vector<std::pair<int32_t, bool>> st{{0, false}};
+    // Post-order of the subtree of `root` (parallel builds interleave node numbering).
+    void post_order(int32_t root, std::vector<int32_t>& order) const {
+        std::vector<std::pair<int32_t, bool>> st{{root, false}};
         while (!st.empty()) {
             auto [v, done] = st.back();
             st.pop_back();
@@ -476,40 +469,85 @@ struct Collapse {
             for (int c = 0; c < 2; ++c)
                 if (t.nodes[v].child[c] >= 0) st.push_back({t.nodes[v].child[c], false});
         }
-        for (int32_t v : order) {
-            const TreeNode<2>& nd = t.nodes[v];
-            const float ca[2] = {box_area(nd.lo[0], nd.hi[0]), box_area(nd.lo[1], nd.hi[1])};
-            BBox b;
-            b.grow(nd.lo[0], nd.hi[0]);
-            b.grow(nd.lo[1], nd.hi[1]);
-            const float av = b.area();
-            prims[v] = count_of(nd.child[0]) + count_of(nd.child[1]);
-            float open[9];
-            uint8_t split[9];
-            for (int k = 2; k <= 8; ++k) {
-                open[k] = INFINITY;
-                split[k] = 1;
-                for (int j = 1; j < k; ++j) {
-                    const float c = cost(nd.child[0], j, ca[0]) + cost(nd.child[1], k - j, ca[1]);
-                    if (c < open[k]) { open[k] = c; split[k] = (uint8_t)j; }
-                }
+    }
+
+    // Subtrees of at most `grain` binary nodes are solved on worker threads,
+    // the nodes above them afterwards in post-order.
+    void run(int threads) {
+        const size_t n = t.nodes.size();
+        best.assign(n * 9, INFINITY);
+        how.assign(n * 9, 0);
+        node_split.assign(n, 4);
+        prims.assign(n, 0);
+        std::vector<int32_t> order;
+        order.reserve(n);
+        post_order(0, order);
+        if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+        const int64_t grain = std::max<int64_t>(8192, (int64_t)n / (8 * (int64_t)threads));
+        if (threads == 1 || (int64_t)n <= 2 * grain) {
+            for (int32_t v : order) solve(v);
+            return;
+        }
+        std::vector<int32_t> size(n, 1);
+        for (int32_t v : order)
+            for (int c = 0; c < 2; ++c)
+                if (t.nodes[v].child[c] >= 0) size[v] += size[t.nodes[v].child[c]];
+        std::vector<int32_t> frontier;
+        std::vector<uint8_t> top(n, 0);
+        std::vector<int32_t> st{0};
+        while (!st.empty()) {
+            const int32_t v = st.back();
+            st.pop_back();
+            if (size[v] <= grain) {
+                frontier.push_back(v);
+                continue;
             }
-            float* bv = &best[(size_t)v * 9];
-            uint8_t* hv = &how[(size_t)v * 9];
-            const float as_node = kNodeCost * av + open[8];
-            node_split[v] = split[8];
-            const float as_leaf = prims[v] <= 3 ? kLeafCost * av * (float)prims[v] : INFINITY;
-            bv[1] = std::min(as_leaf, as_node);
-            hv[1] = as_leaf <= as_node ? 0 : 1;
-            for (int k = 2; k <= 8; ++k) {
-                bv[k] = bv[k - 1];
-                hv[k] = hv[k - 1];
-                if (open[k] < bv[k]) { bv[k] = open[k]; hv[k] = (uint8_t)(2 + split[k]); }
+            top[v] = 1;
+            for (int c = 0; c < 2; ++c)
+                if (t.nodes[v].child[c] >= 0) st.push_back(t.nodes[v].child[c]);
+        }
+        parallel_tasks((int64_t)frontier.size(), threads, [&](int64_t i) {
+            std::vector<int32_t> sub;
+            post_order(frontier[(size_t)i], sub);
+            for (int32_t v : sub) solve(v);
+        });
+        for (int32_t v : order)
+            if (top[v]) solve(v);
+    }
+
+    // best / how / prims of node v from its children's.
+    void solve(int32_t v) {
+        const TreeNode<2>& nd = t.nodes[v];
+        const float ca[2] = {box_area(nd.lo[0], nd.hi[0]), box_area(nd.lo[1], nd.hi[1])};
+        BBox b;
+        b.grow(nd.lo[0], nd.hi[0]);
+        b.grow(nd.lo[1], nd.hi[1]);
+        const float av = b.area();
+        prims[v] = count_of(nd.child[0]) + count_of(nd.child[1]);
+        float open[9];
+        uint8_t split[9];
+        for (int k = 2; k <= 8; ++k) {
+            open[k] = INFINITY;
+            split[k] = 1;
+            for (int j = 1; j < k; ++j) {
+                const float c = cost(nd.child[0], j, ca[0]) + cost(nd.child[1], k - j, ca[1]);
+                if (c < open[k]) { open[k] = c; split[k] = (uint8_t)j; }
             }
+        }
+        float* bv = &best[(size_t)v * 9];
+        uint8_t* hv = &how[(size_t)v * 9];
+        const float as_node = kNodeCost * av + open[8];
+        node_split[v] = split[8];
+        const float as_leaf = prims[v] <= 3 ? kLeafCost * av * (float)prims[v] : INFINITY;
+        bv[1] = std::min(as_leaf, as_node);
+        hv[1] = as_leaf <= as_node ? 0 : 1;
+        for (int k = 2; k <= 8; ++k) {
+            bv[k] = bv[k - 1];
+            hv[k] = hv[k - 1];
+            if (open[k] < bv[k]) { bv[k] = open[k]; hv[k] = (uint8_t)(2 + split[k]); }
         }
     }
 
-    // Triangles of a binary subtree, in leaf order.
     // Triangles of a binary subtree appended to refs, each once from `first` on
     // (fragments of one pre-split triangle can sit in sibling leaves).
     void gather(int32_t code, std::vector<int32_t>& refs, size_t first) const {
@@ -539,18 +577,26 @@ struct Collapse {
 };
 }  // namespace
 
-static void collapse_optimal(const Tree<2>& t2, Tree<8>& out) {
-    Collapse cl(t2);
-    cl.run();
-    out = Tree<8>();
-    out.bounds = t2.bounds;
-    std::vector<std::pair<int32_t, int32_t>> work{{0, 0}};  // (binary node, 8-wide node)
-    out.nodes.push_back(TreeNode<8>{});
+// Emits the 8-wide subtree of binary node `src` into `frag` (its node 0).
+// With split_grain > 0, inner children of at most split_grain triangles are
+// not expanded but listed in `pending` (fragment node, slot, binary node), to
+// be emitted as fragments of their own.
+struct Pending {
+    int32_t node;
+    int slot;
+    int32_t src;
+};
+
+static void emit_subtree(const Collapse& cl, int32_t src, Tree<8>& frag, int64_t split_grain,
+                         std::vector<Pending>* pending) {
+    const Tree<2>& t2 = cl.t;
+    std::vector<std::pair<int32_t, int32_t>> work{{src, 0}};  // (binary node, 8-wide node)
+    frag.nodes.push_back(TreeNode<8>{});
     while (!work.empty()) {
-        const auto [src, dst] = work.back();
+        const auto [s, dst] = work.back();
         work.pop_back();
-        const TreeNode<2>& nd = t2.nodes[src];
-        const int j = cl.node_split[src];  // an 8-wide node opens its binary node into 8 slots
+        const TreeNode<2>& nd = t2.nodes[s];
+        const int j = cl.node_split[s];  // an 8-wide node opens its binary node into 8 slots
         std::vector<Collapse::Child> ch;
         cl.slots(nd.child[0], j, nd.lo[0], nd.hi[0], ch);
         cl.slots(nd.child[1], 8 - j, nd.lo[1], nd.hi[1], ch);
@@ -561,25 +607,73 @@ static void collapse_optimal(const Tree<2>& t2, Tree<8>& out) {
             for (int a = 0; a < 3; ++a) { d.lo[c][a] = ch[c].lo[a]; d.hi[c][a] = ch[c].hi[a]; }
             const int32_t code = ch[c].code;
             if (code >= 0 && cl.how[(size_t)code * 9 + 1] == 1) {
-                const int32_t ni = (int32_t)out.nodes.size();
-                out.nodes.push_back(TreeNode<8>{});
+                if (split_grain > 0 && cl.prims[code] <= split_grain) {
+                    pending->push_back(Pending{dst, (int)c, code});
+                    d.child[c] = 0;  // filled in when the fragments are joined
+                    continue;
+                }
+                const int32_t ni = (int32_t)frag.nodes.size();
+                frag.nodes.push_back(TreeNode<8>{});
                 work.push_back({code, ni});
                 d.child[c] = ni;
             } else {
                 // A binary leaf, or a subtree merged into one leaf (<= 3 triangles).
-                const int32_t first = (int32_t)out.prim_refs.size();
-                cl.gather(code, out.prim_refs, (size_t)first);
-                const int32_t leaf = (int32_t)out.leaves.size();
-                out.leaves.push_back(Leaf{first, (int32_t)out.prim_refs.size() - first});
+                const int32_t first = (int32_t)frag.prim_refs.size();
+                cl.gather(code, frag.prim_refs, (size_t)first);
+                const int32_t leaf = (int32_t)frag.leaves.size();
+                frag.leaves.push_back(Leaf{first, (int32_t)frag.prim_refs.size() - first});
                 d.child[c] = -(leaf + 2);
             }
         }
-        out.nodes[dst] = d;
+        frag.nodes[dst] = d;
     }
 }
 
+// Appends fragment f to out (renumbering its nodes, leaves and references);
+// returns the index its root got.
+static int32_t join_fragment(Tree<8>& out, const Tree<8>& f) {
+    const int32_t node_off = (int32_t)out.nodes.size(), leaf_off = (int32_t)out.leaves.size();
+    const int32_t ref_off = (int32_t)out.prim_refs.size();
+    for (TreeNode<8> nd : f.nodes) {
+        for (int c = 0; c < 8; ++c) {
+            if (nd.child[c] >= 0) nd.child[c] += node_off;
+            else if (nd.child[c] <= -2) nd.child[c] -= leaf_off;
+        }
+        out.nodes.push_back(nd);
+    }
+    for (Leaf l : f.leaves) {
+        l.first += ref_off;
+        out.leaves.push_back(l);
+    }
+    out.prim_refs.insert(out.prim_refs.end(), f.prim_refs.begin(), f.prim_refs.end());
+    return node_off;
+}
 
-void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out) {
+// The 8-wide tree is the same for any thread count (node numbering aside):
+// large trees are emitted as a top fragment plus one fragment per subtree of
+// at most `grain` triangles, converted independently and joined.
+static void collapse_optimal(const Tree<2>& t2, Tree<8>& out, int threads) {
+    Collapse cl(t2);
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    cl.run(threads);
+    out = Tree<8>();
+    out.bounds = t2.bounds;
+    const int64_t total = cl.prims[0];
+    const int64_t grain = std::max<int64_t>(16384, total / (8 * (int64_t)threads));
+    if (threads == 1 || total <= 2 * grain) {
+        emit_subtree(cl, 0, out, 0, nullptr);
+        return;
+    }
+    std::vector<Pending> pending;
+    emit_subtree(cl, 0, out, grain, &pending);
+    std::vector<Tree<8>> frags(pending.size());
+    parallel_tasks((int64_t)pending.size(), threads,
+                   [&](int64_t i) { emit_subtree(cl, pending[(size_t)i].src, frags[(size_t)i], 0, nullptr); });
+    for (size_t i = 0; i < pending.size(); ++i)
+        out.nodes[pending[i].node].child[pending[i].slot] = join_fragment(out, frags[i]);
+}
+
+void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out, int threads) {
     out = Tree<8>();
     out.bounds = t2.bounds;
     out.prim_refs = t2.prim_refs;
@@ -596,7 +690,7 @@ void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out) {
         out.nodes.push_back(r);
         return;
     }
-    collapse_optimal(t2, out);
+    collapse_optimal(t2, out, threads);
 }
 
 template <int W>

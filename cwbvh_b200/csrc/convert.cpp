@@ -231,37 +231,59 @@ int8_t axis_exponent(float extent) {
 
 }  // namespace
 
-template <class EmitPrim>
-static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out);
-
-void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out) {
-    convert_cwbvh_impl(t, [&](int32_t prim) { append_triangle(m, prim, out); }, out);
-}
-
-void convert_cwbvh_instances(const Tree<8>& t, const float* rows12, const int32_t* extra, HostBVH& out) {
-    convert_cwbvh_impl(t, [&](int32_t k) {
-        out.woop.insert(out.woop.end(), rows12 + 12 * (int64_t)k, rows12 + 12 * (int64_t)k + 12);
-        out.prim_index.push_back(k);
-        out.prim_index.push_back(extra[k]);
-        out.prim_index.push_back(-1);
-    }, out);
-}
+// The converter's output order, restated so subtrees can be converted in
+// parallel with identical bytes.  Sequentially, a node's processing appends
+// its inner children's 80 B slots (one contiguous block, in slot order) and
+// its leaf children's triangles (slot order), then pushes the inner children;
+// the stack then converts them last slot first, each subtree completely
+// before the next.  So every subtree owns one contiguous range of node slots
+// and one of triangles, whose starts follow from the subtree sizes: the ranges
+// are computed up front and the subtrees filled independently.
+namespace {
 
 template <class EmitPrim>
-static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out) {
-    out.kind = RQ_BVH_CWBVH;
-    out.nodes.assign(20, 0.0f);  // root slot
-    out.woop.clear();
-    out.prim_index.clear();
-    out.bounds = t.bounds;
+struct CwbvhWriter {
+    const Tree<8>& t;
+    EmitPrim& emit;            // emit(prim, triangle index)
+    HostBVH& out;
+    std::vector<int64_t> desc;  // inner descendants of each node
+    std::vector<int64_t> tris;  // triangles below each node
+    int64_t grain = 0;
+    std::atomic<int> spare{0};
 
-    struct Item { int32_t node; int32_t addr; };  // addr in float4 units
-    std::vector<Item> st{{0, 0}};
-    int64_t n_nodes = 0, n_leaves = 0;
-    while (!st.empty()) {
-        const Item it = st.back();
-        st.pop_back();
-        const TreeNode<8>& nd = t.nodes[it.node];
+    CwbvhWriter(const Tree<8>& tree, EmitPrim& e, HostBVH& o) : t(tree), emit(e), out(o) {}
+
+    void sizes() {
+        const size_t n = t.nodes.size();
+        desc.assign(n, 0);
+        tris.assign(n, 0);
+        std::vector<std::pair<int32_t, bool>> st{{0, false}};
+        while (!st.empty()) {
+            auto [v, done] = st.back();
+            st.pop_back();
+            const TreeNode<8>& nd = t.nodes[v];
+            if (!done) {
+                st.push_back({v, true});
+                for (int c = 0; c < 8; ++c)
+                    if (nd.child[c] >= 0) st.push_back({nd.child[c], false});
+                continue;
+            }
+            for (int c = 0; c < 8; ++c) {
+                const int32_t code = nd.child[c];
+                if (code >= 0) {
+                    desc[v] += 1 + desc[code];
+                    tris[v] += tris[code];
+                } else if (code <= -2) {
+                    tris[v] += t.leaves[-code - 2].count;
+                }
+            }
+        }
+    }
+
+    // Converts node v, whose slot is at float4 `addr`, with its children's
+    // block at float4 `node_cur` and its triangles from `tri_cur` on.
+    void convert(int32_t v, int64_t addr, int64_t node_cur, int64_t tri_cur) {
+        const TreeNode<8>& nd = t.nodes[v];
         Child8 ch[8];
         bool present[8];
         float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -293,43 +315,34 @@ static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out) 
             }
         }
 
-        uint8_t* node_bytes = reinterpret_cast<uint8_t*>(&out.nodes[(size_t)it.addr * 4]);
+        uint8_t* node_bytes = reinterpret_cast<uint8_t*>(&out.nodes[(size_t)addr * 4]);
         uint8_t imask = 0;
-        int32_t child_base = 0, tri_base = 0;
-        int inner = 0, leaf_tris = 0;
+        int64_t inner = 0, leaf_tris = 0;
+        int64_t child_addr[8];
         for (int c = 0; c < 8; ++c) {
+            child_addr[c] = -1;
             if (!op[c]) continue;
-            uint8_t q[6];
             for (int a = 0; a < 3; ++a) {
-                const float scale = std::ldexp(1.0f, e[a]);  // = powf(2, e), exactly
-                q[a] = (uint8_t)(int)std::floor((oc[c].lo[a] - lo[a]) / scale);
-                q[3 + a] = (uint8_t)(int)std::ceil((oc[c].hi[a] - lo[a]) / scale);
+                const float scale = std::ldexp(1.0f, e[a]);
+                node_bytes[32 + c + 8 * a] = (uint8_t)(int)std::floor((oc[c].lo[a] - lo[a]) / scale);
+                node_bytes[32 + c + 8 * (3 + a)] = (uint8_t)(int)std::ceil((oc[c].hi[a] - lo[a]) / scale);
             }
-            // The node buffer may grow below, so address it afresh each time.
-            node_bytes = reinterpret_cast<uint8_t*>(&out.nodes[(size_t)it.addr * 4]);
-            for (int k = 0; k < 6; ++k) node_bytes[32 + c + 8 * k] = q[k];
             uint8_t meta;
             if (oc[c].code >= 0) {
-                const int32_t child_addr = (int32_t)(out.nodes.size() / 4);
-                if (inner == 0) child_base = child_addr / 5;
-                out.nodes.resize(out.nodes.size() + 20, 0.0f);
+                child_addr[c] = node_cur + 5 * inner;
                 imask |= (uint8_t)(1u << c);
                 meta = (uint8_t)((1u << 5) | ((24u + c) & 31u));
                 ++inner;
-                st.push_back({oc[c].code, child_addr});
             } else {
                 const Leaf& lf = t.leaves[-oc[c].code - 2];
-                if (leaf_tris == 0) tri_base = (int32_t)(out.woop.size() / 12);
                 const uint32_t unary = lf.count == 1 ? 1u : (lf.count == 2 ? 3u : 7u);
                 meta = (uint8_t)((unary << 5) | ((uint32_t)leaf_tris & 31u));
+                for (int32_t k = 0; k < lf.count; ++k) emit(t.prim_refs[lf.first + k], tri_cur + leaf_tris + k);
                 leaf_tris += lf.count;
-                for (int32_t k = 0; k < lf.count; ++k) emit(t.prim_refs[lf.first + k]);
-                ++n_leaves;
             }
-            node_bytes = reinterpret_cast<uint8_t*>(&out.nodes[(size_t)it.addr * 4]);
             node_bytes[24 + c] = meta;
         }
-        float* n = &out.nodes[(size_t)it.addr * 4];
+        float* n = &out.nodes[(size_t)addr * 4];
         n[0] = lo[0];
         n[1] = lo[1];
         n[2] = lo[2];
@@ -338,12 +351,74 @@ static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out) 
         w[1] = (uint8_t)e[1];
         w[2] = (uint8_t)e[2];
         w[3] = imask;
-        n[4] = int_bits(child_base);
-        n[5] = int_bits(tri_base);
-        ++n_nodes;
+        n[4] = int_bits(inner ? (int32_t)(node_cur / 5) : 0);
+        n[5] = int_bits(leaf_tris ? (int32_t)tri_cur : 0);
+
+        // Subtrees, last slot first, each in its own ranges.
+        int64_t nc = node_cur + 5 * inner, tc = tri_cur + leaf_tris;
+        std::vector<std::thread> helpers;
+        for (int c = 7; c >= 0; --c) {
+            if (child_addr[c] < 0) continue;
+            const int32_t code = oc[c].code;
+            if (tris[code] >= grain && spare.fetch_sub(1) > 0) {
+                helpers.emplace_back([this, code, a = child_addr[c], nc, tc] { convert(code, a, nc, tc); });
+            } else {
+                if (tris[code] >= grain) spare.fetch_add(1);
+                convert(code, child_addr[c], nc, tc);
+            }
+            nc += 5 * desc[code];
+            tc += tris[code];
+        }
+        for (auto& h : helpers) {
+            h.join();
+            spare.fetch_add(1);
+        }
     }
+};
+
+}  // namespace
+
+template <class EmitPrim>
+static void convert_cwbvh_impl(const Tree<8>& t, EmitPrim&& emit, HostBVH& out, int threads) {
+    out.kind = RQ_BVH_CWBVH;
+    out.bounds = t.bounds;
+    CwbvhWriter<EmitPrim> wr(t, emit, out);
+    wr.sizes();
+    const int64_t n_nodes = 1 + wr.desc[0], n_tris = wr.tris[0];
+    out.nodes.assign((size_t)n_nodes * 20, 0.0f);
+    out.woop.assign((size_t)n_tris * 12, 0.0f);
+    out.prim_index.assign((size_t)n_tris * 3, 0);
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    wr.spare = threads - 1;
+    wr.grain = threads > 1 ? std::max<int64_t>(4096, n_tris / (8 * (int64_t)threads)) : INT64_MAX;
+    wr.convert(0, 0, 5, 0);
+    int64_t n_leaves = 0;
+    for (const TreeNode<8>& nd : t.nodes)
+        for (int c = 0; c < 8; ++c) n_leaves += nd.child[c] <= -2;
     out.node_count = n_nodes;
     out.leaf_count = n_leaves;
+}
+
+void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out, int threads) {
+    auto emit = [&](int32_t prim, int64_t k) {
+        const int32_t* tri = &m.i[3 * (int64_t)prim];
+        woopify(m.vert(tri[0]), m.vert(tri[1]), m.vert(tri[2]), &out.woop[(size_t)k * 12]);
+        out.prim_index[(size_t)k * 3] = prim;
+        out.prim_index[(size_t)k * 3 + 1] = -1;
+        out.prim_index[(size_t)k * 3 + 2] = -1;
+    };
+    convert_cwbvh_impl(t, emit, out, threads);
+}
+
+void convert_cwbvh_instances(const Tree<8>& t, const float* rows12, const int32_t* extra, HostBVH& out,
+                             int threads) {
+    auto emit = [&](int32_t k, int64_t slot) {
+        std::copy(rows12 + 12 * (int64_t)k, rows12 + 12 * (int64_t)k + 12, &out.woop[(size_t)slot * 12]);
+        out.prim_index[(size_t)slot * 3] = k;
+        out.prim_index[(size_t)slot * 3 + 1] = extra[k];
+        out.prim_index[(size_t)slot * 3 + 2] = -1;
+    };
+    convert_cwbvh_impl(t, emit, out, threads);
 }
 
 }  // namespace rq

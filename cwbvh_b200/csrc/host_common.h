@@ -2,9 +2,12 @@
 // produced by the builder and the converted (GPU-layout) buffers.
 #pragma once
 
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
+#include <thread>
 #include <vector>
 
 #include "../../include/rq.h"
@@ -52,6 +55,24 @@ inline uint64_t hash3(uint64_t seed, uint64_t stream, uint64_t i) {
 // Uniform float in [0,1) with 24 random bits.
 inline float u01(uint64_t seed, uint64_t stream, uint64_t i) {
     return (float)(hash3(seed, stream, i) >> 40) * (1.0f / 16777216.0f);
+}
+
+// Runs fn(0 .. n-1) on up to `threads` host threads (0: all cores); each
+// index runs once, in no particular order.
+inline void parallel_tasks(int64_t n, int threads, const std::function<void(int64_t)>& fn) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int workers = (int)std::min<int64_t>(n, threads);
+    if (workers <= 1) {
+        for (int64_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    std::vector<std::thread> pool;
+    for (int w = 0; w < workers; ++w)
+        pool.emplace_back([&] {
+            for (int64_t i = next.fetch_add(1); i < n; i = next.fetch_add(1)) fn(i);
+        });
+    for (auto& th : pool) th.join();
 }
 
 struct Mesh {
@@ -113,18 +134,19 @@ void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool 
 // Binary tree over axis-aligned boxes (lo xyz, hi xyz per box; box k is
 // primitive k), e.g. the world bounds of instances for a top-level tree.
 void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_depth, int threads, Tree<2>& out);
-void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out);
+void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out, int threads = 1);
 int tree_depth2(const Tree<2>& t);
 int tree_depth8(const Tree<8>& t);
 
 // Converters (convert.cpp)
 void woopify(const V3& v0, const V3& v1, const V3& v2, float out[12]);
 void convert_bvh2(const Tree<2>& t, const Mesh& m, HostBVH& out);
-void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out);
+void convert_cwbvh(const Tree<8>& t, const Mesh& m, HostBVH& out, int threads = 1);
 // CWBVH nodes over a tree of instances: each leaf primitive k is emitted as
 // the 3 rows of rows12[12 k ..] (the instance's world-to-object transform) in
 // place of Woop rows, with primitive-map entries (k, extra[k], -1).
-void convert_cwbvh_instances(const Tree<8>& t, const float* rows12, const int32_t* extra, HostBVH& out);
+void convert_cwbvh_instances(const Tree<8>& t, const float* rows12, const int32_t* extra, HostBVH& out,
+                             int threads = 1);
 
 // Scene generators (scenegen.cpp)
 void gen_heightfield_boxes(uint64_t seed, int grid, int n_boxes, float bmin, float bmax, Mesh& m);

@@ -209,3 +209,18 @@ def test_builder_invariants(rq):
     assert 2 * hb.info["depth"] <= 64
     hb2 = rq.HostBVH(V, I, rq.BVH2)
     assert hb2.info["depth"] <= 31
+
+
+@pytest.mark.parametrize("kind", [0, 1], ids=["cwbvh", "bvh2"])
+def test_build_independent_of_thread_count(rq, kind):
+    """The parallel SAH build, 8-wide collapse and conversion give the same
+    bytes as the single-threaded ones (subtrees are emitted into precomputed
+    ranges)."""
+    from cwbvh_b200 import workloads as W
+    V, I = W.scene_of_size(9, 200_000)
+    a = rq.HostBVH(V, I, kind, threads=1)
+    for th in (3, 8):
+        b = rq.HostBVH(V, I, kind, threads=th)
+        assert np.array_equal(a.nodes.view(np.uint32), b.nodes.view(np.uint32))
+        assert np.array_equal(a.woop.view(np.uint32), b.woop.view(np.uint32))
+        assert np.array_equal(a.prim_index, b.prim_index)
