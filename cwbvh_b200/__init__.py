@@ -603,6 +603,21 @@ class Server:
               "rq_server_submit")
         return t.value
 
+    def submit_bake(self, scene_id: int, pos: np.ndarray, nrm: np.ndarray, radius: Optional[np.ndarray],
+                    spp: int, seed: int, tmin: float, tmax: float, offset_scale: float, host_ao: np.ndarray) -> int:
+        """AO bake request: host surfels (pos, nrm (n, 4) float32, radius (n,)
+        or None) in, host_ao (n,) float32 out (occluded / spp); all arrays
+        kept alive by the caller until wait()."""
+        n = pos.shape[0]
+        if nrm.shape[0] != n or host_ao.size < n or (radius is not None and radius.size < n):
+            raise ValueError("pos, nrm, radius and host_ao need one entry per surfel")
+        t = C.c_uint64()
+        check(lib.rq_server_submit_bake(self._h, scene_id, pos.ctypes.data, nrm.ctypes.data,
+                                        radius.ctypes.data if radius is not None else None, n, spp, seed, tmin,
+                                        tmax, offset_scale, host_ao.ctypes.data, C.byref(t)),
+              "rq_server_submit_bake")
+        return t.value
+
     def wait(self, ticket: int, timeout_ms: int = -1) -> dict:
         st = N.RequestStats()
         s = lib.rq_server_wait(self._h, ticket, timeout_ms, C.byref(st))

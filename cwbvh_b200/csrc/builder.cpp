@@ -471,48 +471,44 @@ struct Collapse {
         }
     }
 
-    // Subtrees of at most `grain` binary nodes are solved on worker threads,
-    // the nodes above them afterwards in post-order.
+    // The subtrees below depth D are solved on worker threads (about 8 per
+    // thread for a balanced tree), then the nodes above them in post-order.
     void run(int threads) {
         const size_t n = t.nodes.size();
         best.assign(n * 9, INFINITY);
         how.assign(n * 9, 0);
         node_split.assign(n, 4);
         prims.assign(n, 0);
-        std::vector<int32_t> order;
-        order.reserve(n);
-        post_order(0, order);
         if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-        const int64_t grain = std::max<int64_t>(8192, (int64_t)n / (8 * (int64_t)threads));
-        if (threads == 1 || (int64_t)n <= 2 * grain) {
+        if (threads == 1 || n < 65536) {
+            std::vector<int32_t> order;
+            order.reserve(n);
+            post_order(0, order);
             for (int32_t v : order) solve(v);
             return;
         }
-        std::vector<int32_t> size(n, 1);
-        for (int32_t v : order)
-            for (int c = 0; c < 2; ++c)
-                if (t.nodes[v].child[c] >= 0) size[v] += size[t.nodes[v].child[c]];
-        std::vector<int32_t> frontier;
-        std::vector<uint8_t> top(n, 0);
-        std::vector<int32_t> st{0};
+        int depth_cut = 3;
+        while ((1 << depth_cut) < 8 * threads) ++depth_cut;
+        std::vector<int32_t> frontier, top;  // top: nodes above the cut, in pre-order
+        std::vector<std::pair<int32_t, int>> st{{0, 0}};
         while (!st.empty()) {
-            const int32_t v = st.back();
+            const auto [v, d] = st.back();
             st.pop_back();
-            if (size[v] <= grain) {
+            if (d == depth_cut) {
                 frontier.push_back(v);
                 continue;
             }
-            top[v] = 1;
+            top.push_back(v);
             for (int c = 0; c < 2; ++c)
-                if (t.nodes[v].child[c] >= 0) st.push_back(t.nodes[v].child[c]);
+                if (t.nodes[v].child[c] >= 0) st.push_back({t.nodes[v].child[c], d + 1});
         }
         parallel_tasks((int64_t)frontier.size(), threads, [&](int64_t i) {
             std::vector<int32_t> sub;
             post_order(frontier[(size_t)i], sub);
             for (int32_t v : sub) solve(v);
         });
-        for (int32_t v : order)
-            if (top[v]) solve(v);
+        // Reverse pre-order visits children before parents.
+        for (auto it = top.rbegin(); it != top.rend(); ++it) solve(*it);
     }
 
     // best / how / prims of node v from its children's.

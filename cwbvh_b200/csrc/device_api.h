@@ -46,6 +46,9 @@ struct TraceItem {
     int64_t count;
     uint32_t node_f4;  // node buffer length in float4 (bounds checks)
     uint32_t woop_f4;  // Woop buffer length in float4
+    uint32_t* ao_counts;  // non-null: occluded rays are counted per surfel here instead of writing hits
+    int32_t ao_spp;       // rays per surfel (consecutive) when ao_counts is set
+    int32_t pad;
 };
 
 struct TraceParams {
@@ -60,8 +63,6 @@ struct TraceParams {
     int fetch_nd;
     int fetch_nw;
     int bvh2_speculative;
-    uint32_t* ao_counts;      // non-null: add occluded rays per surfel instead of writing hits
-    int ao_spp;               // rays per surfel (consecutive) when ao_counts is set
 };
 
 typedef void (*TraceKernelFn)(TraceParams);

@@ -333,8 +333,8 @@ static rq_status trace_impl(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, 
     p.total_rays = count;
     p.node_visits = nv;
     p.tri_tests = nt;
-    p.ao_counts = ao_counts;
-    p.ao_spp = ao_spp;
+    p.single.ao_counts = ao_counts;
+    p.single.ao_spp = ao_spp;
     if (speculative >= 0) p.bvh2_speculative = speculative;
     cudaStream_t s = (cudaStream_t)stream;
     rq_status st = reset_counter(ctx, s);

@@ -1,14 +1,18 @@
 // Continuous-batching AO bake server.
 //
-// Requests (scene id, host rays, host hit buffer) queue in arrival order.  A
-// dispatcher thread owns `streams` workers; each worker has device ray/hit
-// arenas of max_batch_rays rays (48 B per ray), so the HBM taken by ray/hit
-// buffers never exceeds streams x max_batch_rays x 48 <= hbm_budget_bytes.
-// Whenever a worker is free, the dispatcher admits the oldest queued requests
-// that fit its arena, copies their rays in, traces all of them in one
-// persistent batch launch and copies the hits back -- all on the worker's
-// stream -- so batches on different workers overlap on the device (the next
-// batch's blocks start as the previous one drains) and copies overlap traces.
+// Requests queue in arrival order.  A ray request is (scene id, host rays,
+// host hit buffer); a bake request is (scene id, host surfels, rays per
+// surfel, host AO buffer): its rays are generated on the device and its
+// occluded rays counted per surfel in the trace epilogue, so only the surfels
+// cross PCIe in and one float per surfel comes back.  A dispatcher thread
+// owns `streams` workers; each worker has one device arena of max_batch_rays
+// x 48 B, so the HBM taken by request buffers never exceeds
+// streams x max_batch_rays x 48 <= hbm_budget_bytes.  Whenever a worker is
+// free, the dispatcher admits the oldest queued requests whose buffers fit
+// its arena, copies their inputs in, traces all of them in one persistent
+// batch launch and copies the results back -- all on the worker's stream --
+// so batches on different workers overlap on the device (the next batch's
+// blocks start as the previous one drains) and copies overlap traces.
 // Requests arriving meanwhile are admitted into the next free worker.
 #include <algorithm>
 #include <chrono>
@@ -37,25 +41,44 @@ bool is_pinned(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
+int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
+
 struct Req {
     uint64_t ticket = 0;
     int32_t scene = 0;
     const rq_ray* host_rays = nullptr;
-    rq_hit* host_hits = nullptr;
-    int64_t count = 0;
+    int64_t count = 0;           // rays
+    // bake requests: surfels in, AO out
+    bool bake = false;
+    const float* host_pos = nullptr;
+    const float* host_nrm = nullptr;
+    const float* host_radius = nullptr;
+    int64_t n_surfels = 0;
+    int spp = 0;
+    uint64_t seed = 0;
+    float tmin = 0.f, tmax = 0.f, offset_scale = 0.f;
+    // result: hits (ray request) or AO per surfel (bake request)
+    void* host_out = nullptr;
+    void* dev_out = nullptr;
+    int64_t out_bytes = 0;
+    int64_t arena_bytes = 0;     // device bytes the request occupies while running
     double submit_ms = 0, start_ms = 0, done_ms = 0;
     int32_t batch = -1;
     rq_status status = RQ_OK;
     enum State { kQueued, kRunning, kDone } state = kQueued;
-    int64_t offset = 0;         // in the worker arena
     bool deferred_copy = false;  // pageable destination: copied after the stream finishes
 };
+
+// Occluded-ray counts of a bake request turned into AO fractions in place.
+__global__ void counts_to_ao_kernel(uint32_t* counts, int64_t n, int spp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) reinterpret_cast<float*>(counts)[i] = (float)counts[i] / (float)spp;
+}
 
 struct Worker {
     cudaStream_t stream = nullptr;
     rq_ctx* ctx = nullptr;
-    rq::Ray* d_rays = nullptr;
-    rq::Hit* d_hits = nullptr;
+    char* d_arena = nullptr;
     rq::TraceItem* d_items = nullptr;
     rq::TraceItem* h_items = nullptr;  // pinned
     std::vector<Req*> inflight;
@@ -69,7 +92,8 @@ constexpr int kMaxItems = 4096;
 
 struct rq_server {
     rq_server_params params{};
-    int64_t cap = 0;
+    int64_t cap = 0;          // rays of a ray request that fill an arena
+    int64_t arena_bytes = 0;  // per worker
     rq_launch launch{};
     rq_bvh_kind kind = RQ_BVH_CWBVH;
     std::vector<rq_scene*> scenes;
@@ -102,38 +126,75 @@ static void CUDART_CB worker_done(void* user) {
 
 void rq_server::launch_batch(Worker& w, std::vector<Req*>& batch, int32_t batch_id) {
     rq_status st = RQ_OK;
-    int64_t off = 0;
+    auto ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == RQ_OK) st = rq::cuda_fail(e, "rq_server batch");
+    };
+    int64_t off = 0, ray_begin = 0;
     for (size_t k = 0; k < batch.size(); ++k) {
         Req* r = batch[k];
-        r->offset = off;
         r->batch = batch_id;
-        if (cudaMemcpyAsync(w.d_rays + off, r->host_rays, (size_t)r->count * sizeof(rq::Ray), cudaMemcpyHostToDevice,
-                            w.stream) != cudaSuccess)
-            st = RQ_ERR_CUDA;
-        rq::TraceItem it = rq::scene_item(scenes[r->scene], (const rq_ray*)(w.d_rays + off), (rq_hit*)(w.d_hits + off),
-                                          r->count);
-        it.ray_begin = off;
+        rq::TraceItem it;
+        if (!r->bake) {
+            rq::Ray* d_rays = reinterpret_cast<rq::Ray*>(w.d_arena + off);
+            off += align256(r->count * (int64_t)sizeof(rq::Ray));
+            rq::Hit* d_hits = reinterpret_cast<rq::Hit*>(w.d_arena + off);
+            off += align256(r->count * (int64_t)sizeof(rq::Hit));
+            ok(cudaMemcpyAsync(d_rays, r->host_rays, (size_t)r->count * sizeof(rq::Ray), cudaMemcpyHostToDevice,
+                               w.stream));
+            it = rq::scene_item(scenes[r->scene], (const rq_ray*)d_rays, (rq_hit*)d_hits, r->count);
+            r->dev_out = d_hits;
+        } else {
+            const int64_t n = r->n_surfels;
+            float* d_pos = reinterpret_cast<float*>(w.d_arena + off);
+            off += align256(16 * n);
+            float* d_nrm = reinterpret_cast<float*>(w.d_arena + off);
+            off += align256(16 * n);
+            float* d_rad = nullptr;
+            if (r->host_radius) {
+                d_rad = reinterpret_cast<float*>(w.d_arena + off);
+                off += align256(4 * n);
+            }
+            uint32_t* d_counts = reinterpret_cast<uint32_t*>(w.d_arena + off);
+            off += align256(4 * n);
+            rq_ray* d_rays = reinterpret_cast<rq_ray*>(w.d_arena + off);
+            off += align256(r->count * (int64_t)sizeof(rq::Ray));
+            ok(cudaMemcpyAsync(d_pos, r->host_pos, (size_t)(16 * n), cudaMemcpyHostToDevice, w.stream));
+            ok(cudaMemcpyAsync(d_nrm, r->host_nrm, (size_t)(16 * n), cudaMemcpyHostToDevice, w.stream));
+            if (d_rad) ok(cudaMemcpyAsync(d_rad, r->host_radius, (size_t)(4 * n), cudaMemcpyHostToDevice, w.stream));
+            ok(cudaMemsetAsync(d_counts, 0, (size_t)(4 * n), w.stream));
+            if (st == RQ_OK)
+                st = rq_aorays(d_pos, d_nrm, d_rad, n, r->spp, r->seed, r->tmin, r->tmax, r->offset_scale, d_rays,
+                               w.stream);
+            it = rq::scene_item(scenes[r->scene], d_rays, nullptr, r->count);
+            it.ao_counts = d_counts;
+            it.ao_spp = r->spp;
+            r->dev_out = d_counts;
+        }
+        it.ray_begin = ray_begin;
+        ray_begin += r->count;
         w.h_items[k] = it;
-        off += r->count;
     }
-    if (st == RQ_OK && cudaMemcpyAsync(w.d_items, w.h_items, batch.size() * sizeof(rq::TraceItem),
-                                       cudaMemcpyHostToDevice, w.stream) != cudaSuccess)
-        st = RQ_ERR_CUDA;
+    if (st == RQ_OK)
+        ok(cudaMemcpyAsync(w.d_items, w.h_items, batch.size() * sizeof(rq::TraceItem), cudaMemcpyHostToDevice,
+                           w.stream));
     if (st == RQ_OK) st = rq::reset_counter(w.ctx, w.stream);
     if (st == RQ_OK) {
         rq::TraceParams p = rq::base_params(w.ctx, launch);
         p.single = w.h_items[0];
         p.items = w.d_items;
         p.n_items = (int)batch.size();
-        p.total_rays = off;
+        p.total_rays = ray_begin;
         st = rq::launch_trace(kind, params.query, launch, true, false, p, w.stream);
     }
     for (Req* r : batch) {
-        r->deferred_copy = !is_pinned(r->host_hits);
-        if (st == RQ_OK && !r->deferred_copy &&
-            cudaMemcpyAsync(r->host_hits, w.d_hits + r->offset, (size_t)r->count * sizeof(rq::Hit),
-                            cudaMemcpyDeviceToHost, w.stream) != cudaSuccess)
-            st = RQ_ERR_CUDA;
+        if (r->bake && st == RQ_OK) {
+            counts_to_ao_kernel<<<(unsigned)((r->n_surfels + 255) / 256), 256, 0, w.stream>>>(
+                (uint32_t*)r->dev_out, r->n_surfels, r->spp);
+            ok(cudaGetLastError());
+        }
+        r->deferred_copy = !is_pinned(r->host_out);
+        if (st == RQ_OK && !r->deferred_copy)
+            ok(cudaMemcpyAsync(r->host_out, r->dev_out, (size_t)r->out_bytes, cudaMemcpyDeviceToHost, w.stream));
     }
     for (Req* r : batch) r->status = st;
     w.inflight = batch;
@@ -152,8 +213,7 @@ void rq_server::finalize(Worker& w) {
     rq_status kst = rq_ctx_check(w.ctx, w.stream);
     for (Req* r : w.inflight) {
         if (r->status == RQ_OK && r->deferred_copy &&
-            cudaMemcpy(r->host_hits, w.d_hits + r->offset, (size_t)r->count * sizeof(rq::Hit),
-                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            cudaMemcpy(r->host_out, r->dev_out, (size_t)r->out_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
             r->status = RQ_ERR_CUDA;
         if (r->status == RQ_OK) r->status = kst;
     }
@@ -200,11 +260,12 @@ void rq_server::run() {
         for (auto& w : workers) {
             if (w.busy || pending.empty()) continue;
             std::vector<Req*> batch;
-            int64_t rays = 0;
-            while (!pending.empty() && (int)batch.size() < kMaxItems && rays + pending.front()->count <= cap) {
+            int64_t bytes = 0;
+            while (!pending.empty() && (int)batch.size() < kMaxItems &&
+                   bytes + pending.front()->arena_bytes <= arena_bytes) {
                 Req* r = pending.front();
                 pending.pop_front();
-                rays += r->count;
+                bytes += r->arena_bytes;
                 batch.push_back(r);
             }
             if (batch.empty()) continue;
@@ -234,6 +295,7 @@ rq_status rq_server_create(const rq_server_params* params, rq_server_t* out) {
     int64_t cap = params->hbm_budget_bytes / (48 * (int64_t)streams);
     if (params->max_batch_rays > 0) cap = std::min(cap, params->max_batch_rays);
     s->cap = cap;
+    s->arena_bytes = 48 * cap + 512;  // + two 256-B alignment pads: a ray request of `cap` rays fits
     if (cap <= 0) {
         delete s;
         return RQ_ERR_INVALID_ARG;
@@ -246,8 +308,7 @@ rq_status rq_server_create(const rq_server_params* params, rq_server_t* out) {
         if (e == cudaSuccess) st = rq_ctx_create(&w.ctx);
         else st = rq::cuda_fail(e, "rq_server_create");
         if (st != RQ_OK) break;
-        e = cudaMalloc(&w.d_rays, (size_t)cap * sizeof(rq::Ray));
-        if (e == cudaSuccess) e = cudaMalloc(&w.d_hits, (size_t)cap * sizeof(rq::Hit));
+        e = cudaMalloc(&w.d_arena, (size_t)s->arena_bytes);
         if (e == cudaSuccess) e = cudaMalloc(&w.d_items, kMaxItems * sizeof(rq::TraceItem));
         if (e == cudaSuccess) e = cudaMallocHost(&w.h_items, kMaxItems * sizeof(rq::TraceItem));
         if (e != cudaSuccess) st = rq::cuda_fail(e, "rq_server_create");
@@ -275,29 +336,18 @@ rq_status rq_server_add_scene(rq_server_t s, rq_scene_t scene, int32_t* scene_id
     return RQ_OK;
 }
 
-rq_status rq_server_submit(rq_server_t s, int32_t scene_id, const rq_ray* host_rays, rq_hit* host_hits, int64_t count,
-                           uint64_t* ticket) {
-    if (!s || !host_rays || !host_hits || count <= 0 || !ticket) return RQ_ERR_INVALID_ARG;
-    Req* r = new Req();
+static rq_status enqueue(rq_server_t s, Req* r, uint64_t* ticket) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        if (s->stop) {
+        rq_status st = RQ_OK;
+        if (s->stop) st = RQ_ERR_CANCELLED;
+        else if (r->scene < 0 || r->scene >= (int32_t)s->scenes.size()) st = RQ_ERR_NOT_FOUND;
+        else if (r->arena_bytes > s->arena_bytes) st = RQ_ERR_BUDGET;
+        if (st != RQ_OK) {
             delete r;
-            return RQ_ERR_CANCELLED;
-        }
-        if (scene_id < 0 || scene_id >= (int32_t)s->scenes.size()) {
-            delete r;
-            return RQ_ERR_NOT_FOUND;
-        }
-        if (count > s->cap) {
-            delete r;
-            return RQ_ERR_BUDGET;
+            return st;
         }
         r->ticket = s->next_ticket++;
-        r->scene = scene_id;
-        r->host_rays = host_rays;
-        r->host_hits = host_hits;
-        r->count = count;
         r->submit_ms = now_ms();
         s->reqs[r->ticket] = r;
         s->pending.push_back(r);
@@ -305,6 +355,46 @@ rq_status rq_server_submit(rq_server_t s, int32_t scene_id, const rq_ray* host_r
     }
     s->cv.notify_all();
     return RQ_OK;
+}
+
+rq_status rq_server_submit(rq_server_t s, int32_t scene_id, const rq_ray* host_rays, rq_hit* host_hits, int64_t count,
+                           uint64_t* ticket) {
+    if (!s || !host_rays || !host_hits || count <= 0 || !ticket) return RQ_ERR_INVALID_ARG;
+    Req* r = new Req();
+    r->scene = scene_id;
+    r->host_rays = host_rays;
+    r->count = count;
+    r->host_out = host_hits;
+    r->out_bytes = count * (int64_t)sizeof(rq::Hit);
+    r->arena_bytes = align256(count * (int64_t)sizeof(rq::Ray)) + align256(count * (int64_t)sizeof(rq::Hit));
+    return enqueue(s, r, ticket);
+}
+
+rq_status rq_server_submit_bake(rq_server_t s, int32_t scene_id, const float* host_pos, const float* host_nrm,
+                                const float* host_radius, int64_t n_surfels, int spp, uint64_t seed, float tmin,
+                                float tmax, float offset_scale, float* host_ao, uint64_t* ticket) {
+    if (!s || !host_pos || !host_nrm || !host_ao || n_surfels <= 0 || spp <= 0 || !ticket ||
+        n_surfels > INT64_MAX / 64 / spp)
+        return RQ_ERR_INVALID_ARG;
+    if (s->params.query != RQ_ANY) return RQ_ERR_INVALID_ARG;  // AO counts need the any-hit kernels
+    Req* r = new Req();
+    r->scene = scene_id;
+    r->bake = true;
+    r->host_pos = host_pos;
+    r->host_nrm = host_nrm;
+    r->host_radius = host_radius;
+    r->n_surfels = n_surfels;
+    r->spp = spp;
+    r->seed = seed;
+    r->tmin = tmin;
+    r->tmax = tmax;
+    r->offset_scale = offset_scale;
+    r->count = n_surfels * spp;
+    r->host_out = host_ao;
+    r->out_bytes = 4 * n_surfels;
+    r->arena_bytes = 2 * align256(16 * n_surfels) + (host_radius ? align256(4 * n_surfels) : 0) +
+                     align256(4 * n_surfels) + align256(r->count * (int64_t)sizeof(rq::Ray));
+    return enqueue(s, r, ticket);
 }
 
 rq_status rq_server_wait(rq_server_t s, uint64_t ticket, int64_t timeout_ms, rq_request_stats* stats) {
@@ -363,8 +453,7 @@ rq_status rq_server_destroy(rq_server_t s) {
     for (auto& w : s->workers) {
         if (w.stream) cudaStreamSynchronize(w.stream);
         if (w.ctx) rq_ctx_destroy(w.ctx);
-        cudaFree(w.d_rays);
-        cudaFree(w.d_hits);
+        cudaFree(w.d_arena);
         cudaFree(w.d_items);
         if (w.h_items) cudaFreeHost(w.h_items);
         if (w.stream) cudaStreamDestroy(w.stream);

@@ -36,9 +36,9 @@ constexpr uint32_t kBvh2Sentinel = 0x76543210u;  // src/TraversalKernelBVH2.cu:3
 struct Lane {
     const float4* nodes;
     const float4* woop;
-    Hit* hits;
     int64_t out_idx;
     int64_t gidx;
+    int item;  // batch item of the ray (its hit buffer or AO counters are read at the end)
     uint32_t node_f4, woop_f4;
 };
 
@@ -52,11 +52,11 @@ __device__ __forceinline__ Ray fetch_ray(const TraceParams& p, int64_t g, Lane& 
             if (p.items[mid].ray_begin <= g) lo = mid; else hi = mid - 1;
         }
         it = p.items + lo;
+        L.item = lo;
     }
     const int64_t local = g - (MULTI ? it->ray_begin : 0);
     L.nodes = it->nodes;
     L.woop = it->woop;
-    L.hits = it->hits;
     L.node_f4 = it->node_f4;
     L.woop_f4 = it->woop_f4;
     L.out_idx = it->perm ? (int64_t)__ldg(it->perm + local) : local;
@@ -69,6 +69,19 @@ __device__ __forceinline__ Ray fetch_ray(const TraceParams& p, int64_t g, Lane& 
 
 __device__ __forceinline__ void store_hit(Hit* hits, int64_t i, float t, int addr, float u, float v) {
     __stcs(&hits[i].t_triId_u_v, make_float4(t, __int_as_float(addr), u, v));
+}
+
+// A finished ray's result: its Hit, or -- for an item with AO counters -- one
+// count for its surfel when it is occluded.
+template <bool MULTI>
+__device__ __forceinline__ void finish_ray(const TraceParams& p, const Lane& L, float t, int addr, float u, float v) {
+    const TraceItem* it = MULTI ? p.items + L.item : &p.single;
+    uint32_t* counts = it->ao_counts;
+    if (counts) {
+        if (addr >= 0) atomicAdd(counts + L.out_idx / it->ao_spp, 1u);
+    } else {
+        store_hit(it->hits, L.out_idx, t, addr, u, v);
+    }
 }
 
 // ------------------------------------------------------------------ CWBVH --
@@ -108,11 +121,7 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
             atomicOr(&p.scratch->error, err);
             hit_addr = -1;
         }
-        if (p.ao_counts) {
-            if (hit_addr >= 0) atomicAdd(p.ao_counts + L.out_idx / p.ao_spp, 1u);
-        } else {
-            store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
-        }
+        finish_ray<MULTI>(p, L, tmax, hit_addr, hu, hv);
         if (COUNT) {
             p.node_visits[L.gidx] = nvis;
             p.tri_tests[L.gidx] = ntri;
@@ -277,11 +286,7 @@ __global__ void RQ_KERNEL_BOUNDS bvh2_kernel(const TraceParams p) {
             atomicOr(&p.scratch->error, err);
             hit_addr = -1;
         }
-        if (p.ao_counts) {
-            if (hit_addr >= 0) atomicAdd(p.ao_counts + L.out_idx / p.ao_spp, 1u);
-        } else {
-            store_hit(L.hits, L.out_idx, tmax, hit_addr, hu, hv);
-        }
+        finish_ray<MULTI>(p, L, tmax, hit_addr, hu, hv);
         if (COUNT) {
             p.node_visits[L.gidx] = nvis;
             p.tri_tests[L.gidx] = ntri;

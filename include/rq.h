@@ -360,6 +360,19 @@ rq_status rq_server_add_scene(rq_server_t server, rq_scene_t scene, int32_t* sce
 rq_status rq_server_submit(rq_server_t server, int32_t scene_id, const rq_ray* host_rays,
                            rq_hit* host_hits, int64_t count, uint64_t* ticket);
 /* timeout_ms < 0 waits without limit. */
+/* An AO bake request: n_surfels host surfels (pos, nrm float4 each, radius
+ * float each or NULL for 0) and `spp` rays per surfel generated on the device
+ * exactly as rq_aorays does (seed, tmin, tmax, offset_scale), traced any-hit
+ * with the occluded rays counted per surfel in the trace epilogue; host_ao
+ * (n_surfels floats) receives occluded / spp, equal to rq_aorays + rq_trace
+ * + rq_ao_reduce.  Only the surfels (36 B each) go to the device and 4 B per
+ * surfel come back.  The request occupies 36 B per surfel + 4 B per surfel +
+ * 32 B per ray of arena (rounded to 256 B per buffer); RQ_ERR_BUDGET if that
+ * exceeds one worker's arena, RQ_ERR_INVALID_ARG on a closest-hit server. */
+rq_status rq_server_submit_bake(rq_server_t server, int32_t scene_id, const float* host_pos,
+                                const float* host_nrm, const float* host_radius, int64_t n_surfels,
+                                int spp, uint64_t seed, float tmin, float tmax, float offset_scale,
+                                float* host_ao, uint64_t* ticket);
 rq_status rq_server_wait(rq_server_t server, uint64_t ticket, int64_t timeout_ms,
                          rq_request_stats* stats);
 rq_status rq_server_cancel(rq_server_t server, uint64_t ticket);

@@ -127,3 +127,68 @@ def test_failures_are_status_codes(rq, scenes):
             srv.wait(tickets[-1])
         assert e.value.status == 9  # RQ_ERR_CANCELLED
     srv.close()
+
+
+def _surfels(rq, ds, n, seed):
+    pos, nrm, rad = rq.sample_surfels(ds.vertices, ds.indices, n, seed)
+    rad.fill_(0.001)
+    return pos.cpu().numpy(), nrm.cpu().numpy(), rad.cpu().numpy()
+
+
+def test_bake_requests_equal_trace_then_reduce(rq, scenes):
+    """A bake request (surfels in, AO out; rays generated and counted on the
+    device) gives exactly rq_aorays + rq_trace any-hit + rq_ao_reduce, alone
+    and mixed with ray requests in the same batches."""
+    import torch
+    from cwbvh_b200 import workloads as W
+    srv = rq.Server(hbm_budget_bytes=1 << 30, query=rq.ANY, streams=2)
+    ids = [srv.add_scene(ds.scene) for ds in scenes]
+    ctx = rq.Context()
+    jobs = []
+    for k in range(9):
+        sid, spp = k % len(scenes), (1, 8, 32)[k % 3]
+        n = 3000 + 1500 * k
+        pos, nrm, rad = _surfels(rq, scenes[sid], n, 40 + k)
+        rad = rad if k % 4 else None  # radius-less requests too
+        dg = scenes[sid].diag
+        args = (spp, 500 + k, 1e-4 * dg, 0.1 * dg, 0.5)
+        rays = rq.aorays(torch.from_numpy(pos).cuda(), torch.from_numpy(nrm).cuda(),
+                         torch.from_numpy(rad).cuda() if rad is not None else None,
+                         spp, seed=args[1], tmin=args[2], tmax=args[3], offset_scale=args[4])
+        hits = torch.empty((rays.shape[0], 4), device="cuda")
+        rq.trace(ctx, scenes[sid].scene, rays, hits, rq.ANY)
+        want = rq.ao_reduce(hits, n, spp).cpu().numpy()
+        ao = _pinned((n,)) if k % 2 else np.zeros(n, np.float32)  # pinned and pageable results
+        jobs.append((sid, pos, nrm, rad, args, ao, want, n))
+    ctx.check()
+    mixed_rays = [(k % len(scenes), _pinned((20000, 8))) for k in range(4)]
+    for k, (sid, r) in enumerate(mixed_rays):
+        r[:] = _rays(W, scenes[sid], 20000, 900 + k)
+    tickets = []
+    for j, (sid, pos, nrm, rad, args, ao, want, n) in enumerate(jobs):
+        tickets.append(srv.submit_bake(ids[sid], pos, nrm, rad, *args, ao))
+        if j < len(mixed_rays):
+            sid2, r = mixed_rays[j]
+            tickets.append(srv.submit(ids[sid2], r, _pinned((20000, 4))))
+    stats = [srv.wait(t) for t in tickets]
+    assert all(s["status"] == 0 for s in stats)
+    for sid, pos, nrm, rad, args, ao, want, n in jobs:
+        assert np.array_equal(ao, want)
+    assert any(0.0 < float(j[5].mean()) < 1.0 for j in jobs)
+    srv.close()
+
+
+def test_bake_request_errors(rq, scenes):
+    pos = np.zeros((10, 4), np.float32)
+    ao = np.zeros(10, np.float32)
+    closest = rq.Server(hbm_budget_bytes=1 << 26, query=rq.CLOSEST)
+    cid = closest.add_scene(scenes[0].scene)
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        closest.submit_bake(cid, pos, pos, None, 4, 0, 0.0, 1.0, 0.0, ao)
+    closest.close()
+    small = rq.Server(hbm_budget_bytes=48 * 3000, query=rq.ANY, streams=1)
+    sid = small.add_scene(scenes[0].scene)
+    big = np.zeros((200, 4), np.float32)
+    with pytest.raises(rq.RQError, match="BUDGET"):
+        small.submit_bake(sid, big, big, None, 32, 0, 0.0, 1.0, 0.0, np.zeros(200, np.float32))
+    small.close()
