@@ -43,7 +43,7 @@ class RQError(RuntimeError):
 
 class Launch(C.Structure):
     _fields_ = [("block_size", C.c_int), ("blocks_per_sm", C.c_int), ("smem_stack", C.c_int),
-                ("postpone_ratio", f32), ("fetch_nd", C.c_int), ("fetch_nw", C.c_int)]
+                ("postpone_ratio", f32), ("fetch_nd", C.c_int), ("fetch_nw", C.c_int), ("step_limit", C.c_int)]
 
 
 class BuildParams(C.Structure):

@@ -27,6 +27,8 @@ enum : unsigned {
 };
 
 // Device scratch of one context: the dynamic-fetch counter and the error word.
+constexpr int kDefaultStepLimit = 1 << 22;  // node visits per ray before kErrTimeout (rq_launch.step_limit = 0)
+
 struct DevScratch {
     unsigned long long ray_counter;
     unsigned int error;
@@ -63,6 +65,7 @@ struct TraceParams {
     int fetch_nd;
     int fetch_nw;
     int bvh2_speculative;
+    int step_limit;           // node visits per ray before kErrTimeout
 };
 
 typedef void (*TraceKernelFn)(TraceParams);

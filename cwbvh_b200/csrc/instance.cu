@@ -46,6 +46,7 @@ struct InstParams {
     DevScratch* scratch;
     float postpone_ratio;       // triangle / instance postponing (0: the oracle's order)
     int fetch_nd, fetch_nw;
+    int step_limit;             // node visits per ray (both levels) before kErrTimeout
 };
 
 namespace {
@@ -173,7 +174,7 @@ __global__ void __launch_bounds__(128, 8) cwbvh_inst_kernel(const InstParams p) 
                     if (ng.y > 0x00FFFFFFu && !push(ng)) fault = kErrStackOverflow;
                     const unsigned slot = (bit - 24u) ^ octinv;
                     const unsigned ci = base + (unsigned)__popc(hitsm & ~(0xFFFFFFFFu << slot));
-                    if (++steps > kStepLimit) fault |= kErrTimeout;
+                    if (++steps > p.step_limit) fault |= kErrTimeout;
                     if ((uint64_t)ci * 5u + 5u > (uint64_t)node_f4) fault |= kErrBadScene;
                     if (!fault) cwbvh_visit(nodes + (size_t)ci * 5u, ox, oy, oz, idx_, idy, idz, octinv4, tmin, tmax,
                                             ng, tg);
@@ -370,6 +371,7 @@ rq_status rq_trace_instanced(rq_ctx_t ctx, rq_tlas_t tlas, const rq_ray* rays, r
     p.postpone_ratio = launch && launch->postpone_ratio > 0.f ? l.postpone_ratio : 0.f;
     p.fetch_nd = l.fetch_nd;
     p.fetch_nw = l.fetch_nw;
+    p.step_limit = l.step_limit;
     constexpr int kSmem = 8, kBlock = 128;
     void (*fn)(InstParams) = query == RQ_ANY ? cwbvh_inst_kernel<true, kSmem> : cwbvh_inst_kernel<false, kSmem>;
     const size_t smem = (size_t)kSmem * kBlock * sizeof(uint2);

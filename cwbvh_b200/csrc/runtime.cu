@@ -44,6 +44,7 @@ rq_launch resolve_launch(rq_bvh_kind kind, rq_query q, const rq_launch* l) {
     // than the reference's Nd = 4, Nw = 16 (src/TraversalKernelCWBVH.cu:366-367).
     r.fetch_nd = 0;
     r.fetch_nw = 1;
+    r.step_limit = kDefaultStepLimit;
     (void)q;
     if (l) {
         if (l->block_size > 0) r.block_size = l->block_size;
@@ -53,6 +54,7 @@ rq_launch resolve_launch(rq_bvh_kind kind, rq_query q, const rq_launch* l) {
         if (l->postpone_ratio < 0.f) r.postpone_ratio = 0.f;  // negative: postponing off
         if (l->fetch_nd > 0) r.fetch_nd = l->fetch_nd;
         if (l->fetch_nw > 0) r.fetch_nw = l->fetch_nw;
+        if (l->step_limit > 0) r.step_limit = l->step_limit;
     }
     // Below 1, so the lanes still holding triangles always include enough of
     // the warp to go ahead instead of postponing again.
@@ -130,6 +132,7 @@ TraceParams base_params(rq_ctx* ctx, const rq_launch& l) {
     p.fetch_nd = l.fetch_nd;
     p.fetch_nw = l.fetch_nw;
     p.bvh2_speculative = 1;
+    p.step_limit = l.step_limit;
     return p;
 }
 

@@ -13,7 +13,7 @@
 // every loop is warp-uniform, so lanes never diverge around a collective.
 //
 // Safety.  A ray whose stack would overflow, whose node/triangle index falls
-// outside the buffers, or that runs more than kStepLimit steps is finished as
+// outside the buffers, or that runs more than the step limit is finished as
 // a miss and the context's error word records why; the kernel itself never
 // reads outside the buffers it was given and never spins without a bound.
 #include <cstdio>
@@ -173,7 +173,7 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
                     if (ng.y > 0x00FFFFFFu && !push(ng)) fault = kErrStackOverflow;
                     const unsigned slot = (bit - 24u) ^ octinv;
                     const unsigned ci = base + (unsigned)__popc(hitsm & ~(0xFFFFFFFFu << slot));
-                    if (++steps > kStepLimit) fault |= kErrTimeout;
+                    if (++steps > p.step_limit) fault |= kErrTimeout;
                     if ((uint64_t)ci * 5u + 5u > (uint64_t)L.node_f4) fault |= kErrBadScene;
                     if (!fault) {
                         const float4* np = L.nodes + (size_t)ci * 5u;
@@ -332,7 +332,7 @@ __global__ void RQ_KERNEL_BOUNDS bvh2_kernel(const TraceParams p) {
                 if (__ballot_sync(kFullMask, in) == 0u) break;
                 if (in) {
                     unsigned fault = 0u;
-                    if (++steps > kStepLimit) fault |= kErrTimeout;
+                    if (++steps > p.step_limit) fault |= kErrTimeout;
                     if ((uint64_t)(unsigned)node + 4u > (uint64_t)L.node_f4) fault |= kErrBadScene;
                     if (!fault) {
                         const float4* np = L.nodes + node;

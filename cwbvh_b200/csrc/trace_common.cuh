@@ -22,7 +22,6 @@ namespace rq {
 
 constexpr unsigned kFullMask = 0xFFFFFFFFu;
 constexpr float kOoeps = 0x1p-80f;           // 2^-80, src/TraversalKernelCWBVH.cu:31
-constexpr int kStepLimit = 1 << 22;           // per-ray traversal steps before kErrTimeout
 
 __device__ __forceinline__ unsigned lanemask_lt() {
     unsigned m;

@@ -66,6 +66,7 @@ typedef struct rq_launch {
     float postpone_ratio; /* triangle postponing threshold Rt (reference 0.2)   */
     int fetch_nd;         /* dynamic fetch: idle lanes tolerated (default 0, reference 4)       */
     int fetch_nw;         /* dynamic fetch: lost-iteration budget (default 1, reference 16)     */
+    int step_limit;       /* node visits per ray before it ends with RQ_ERR_TIMEOUT (0 = 2^22) */
 } rq_launch;
 
 /* --------------------------------------------------- host BVH construction */
@@ -491,7 +492,7 @@ rq_status rq_tlas_buffers(rq_tlas_t tlas, const float** nodes, int64_t* node_flo
                           const float** rows, int64_t* row_float4s, const int32_t** map);
 /* launch: NULL for the defaults; only postpone_ratio (triangle / instance
  * postponing as in rq_trace, but off unless a positive ratio is given: off is
- * the oracle's traversal order) and fetch_nd / fetch_nw are used. */
+ * the oracle's traversal order), fetch_nd / fetch_nw and step_limit are used. */
 rq_status rq_trace_instanced(rq_ctx_t ctx, rq_tlas_t tlas, const rq_ray* rays, rq_hit* hits,
                              int32_t* instance_out, int64_t count, rq_query query,
                              const rq_launch* launch, void* stream);
