@@ -185,6 +185,46 @@ def measure_l2_read(stream, mbytes: int = 48, reps: int = 100) -> float:
     return n * reps / (ms * 1e-3) / 1e9
 
 
+def measure_link(mbytes: int = 1024) -> dict:
+    """Host link bandwidth with pinned buffers: H2D alone, D2H alone and both
+    directions at once on two streams (GB/s), 1 GiB copies."""
+    import torch
+    n = mbytes << 20
+    h = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    h2 = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(n, dtype=torch.uint8, device="cuda")
+    d2 = torch.empty(n, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps
+
+    def both():
+        with torch.cuda.stream(s1):
+            d.copy_(h, non_blocking=True)
+        with torch.cuda.stream(s2):
+            h2.copy_(d2, non_blocking=True)
+    h2d = n / timed(lambda: d.copy_(h, non_blocking=True)) / 1e9
+    d2h = n / timed(lambda: h2.copy_(d2, non_blocking=True)) / 1e9
+    duplex = 2 * n / timed(both) / 1e9
+    return {"h2d_gbs": round(h2d, 1), "d2h_gbs": round(d2h, 1), "duplex_gbs": round(duplex, 1)}
+
+
+def link_bound_ms(h2d_bytes: float, d2h_bytes: float, link: dict) -> float:
+    """Least time to move the bytes: the two directions overlap at the duplex
+    rate (half each) until the smaller is done, then the rest one way."""
+    each = link["duplex_gbs"] / 2 * 1e9
+    small, big = sorted((h2d_bytes, d2h_bytes))
+    rest_rate = (link["h2d_gbs"] if h2d_bytes >= d2h_bytes else link["d2h_gbs"]) * 1e9
+    return (small / each + (big - small) / rest_rate) * 1e3
+
+
 def profile_traffic(workload: str):
     """DRAM bytes per launch of the trace kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"traffic_{workload}.json"
@@ -412,6 +452,8 @@ def main():
     achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
     traffic = profile_traffic(args.workload + ("_quick" if args.quick else ""))
     l2_gbs = measure_l2_read(stream)
+    link = measure_link()
+    link_ms = link_bound_ms(total_rays * 32, total_rays * 16, link)
 
     # ---- the reference's CWBVH kernel rebuilt for sm_100a, same rays (closest-hit: its only mode)
     ref_gpu = None
@@ -479,7 +521,12 @@ def main():
                         "host wall clock with the device idle on both sides",
                 "single_stream": {"value": round(world_rays / (ms_e2e * 1e-3) / 1e6, 2),
                                   "ms_per_step": round(ms_e2e, 4),
-                                  "path": "H2D rays + rq_batch_run + D2H hits on one stream, CUDA events"}},
+                                  "path": "H2D rays + rq_batch_run + D2H hits on one stream, CUDA events"},
+                "link": dict(link, bound_ms_per_step=round(link_ms, 3),
+                             bound_mrays_per_s=round(total_rays / (link_ms * 1e-3) / 1e6, 1),
+                             frac=round(link_ms / max(ms_e2e_served, 1e-9), 4),
+                             what="host link measured in this run (pinned 1 GiB copies); bound = least time to move "
+                                  "this step's H2D and D2H bytes")},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": f"hbm_gbs of {peak_kind}",
                      "traffic": (traffic or {}).get("dram_bytes_per_launch"),
