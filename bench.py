@@ -1071,9 +1071,10 @@ def run_large(args, world, rank, dist):
     if args.rays:
         n_surf = max(1, args.rays // 4)
     spp = 4
-    t0 = time.time()
     V, I = rq.gen_spheres_terrain(rank, n_tris)
+    t0 = time.time()
     hb = rq.HostBVH(V, I, rq.CWBVH)
+    t_host_build = time.time() - t0
     log(f"[bench] large {I.shape[0]/1e6:.1f}M tris built in {time.time()-t0:.1f}s "
         f"(nodes {hb.nodes.nbytes/1e9:.2f} GB, woop {hb.woop.nbytes/1e9:.2f} GB)")
     stream = torch.cuda.Stream()
@@ -1086,7 +1087,7 @@ def run_large(args, world, rank, dist):
         dg = W.diag(V)
         rays = rq.aorays(pos, nrm, rad, spp, seed=rank + 2000, tmin=1e-4 * dg, tmax=0.1 * dg, offset_scale=0.0,
                          stream=stream)
-        del pos, nrm, rad, v, i
+        del pos, nrm, rad
         n = rays.shape[0]
         hits = torch.empty((n, 4), device="cuda")
         shits = torch.empty((n, 4), device="cuda")
@@ -1099,6 +1100,21 @@ def run_large(args, world, rank, dist):
         return
     ms_plain = time_steps(lambda: rq.trace(ctx, sc, rays, hits, rq.ANY, stream=stream), args.steps, warmup, stream,
                           dist)
+    # the same mesh built on the GPU (linear BVH collapsed to CWBVH): build time and trace speed
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gsc = rq.Scene.build_gpu(v, i, stream=stream)
+    torch.cuda.synchronize()
+    t_gpu_build = time.perf_counter() - t0
+    del v, i
+    with torch.cuda.stream(stream):
+        ghits = torch.empty((n, 4), device="cuda")
+    ms_gpu_tree = time_steps(lambda: rq.trace(ctx, gsc, rays, ghits, rq.ANY, stream=stream), args.steps, warmup,
+                             stream, dist)
+    ctx.check(stream)
+    torch.cuda.synchronize()
+    gpu_same = float(((ghits[:, 1].view(torch.int32) != -1) == (hits[:, 1].view(torch.int32) != -1)).float().mean())
+    del ghits, gsc
     with torch.cuda.stream(stream):
         occl = torch.zeros(n // spp, dtype=torch.int32, device="cuda")
 
@@ -1129,6 +1145,10 @@ def run_large(args, world, rank, dist):
                    "fused_ao_counts": dict(_pass("fused", n, ms_fused),
                                            what="rq_trace_ao: per-surfel occluded counts in the trace epilogue, "
                                                 "no hit buffer (memset of the counts included)")},
+        "gpu_built_tree": {"build_s": round(t_gpu_build, 3), "host_build_s": round(t_host_build, 2),
+                           "mrays_per_s": round(n / (ms_gpu_tree * 1e-3) / 1e6, 2),
+                           "occlusion_same_frac": round(gpu_same, 6),
+                           "what": "rq_build_scene_gpu: Morton-ordered linear BVH collapsed to CWBVH on the device"},
         "sorted_occlusion_identical": same, "fused_counts_identical": fused_same,
         "ao_occluded_fraction": round(occ, 4),
         "triangles": int(I.shape[0]), "scene_bytes": int(hb.nodes.nbytes + hb.woop.nbytes),

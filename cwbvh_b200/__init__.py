@@ -283,6 +283,32 @@ class Scene:
         return cls(h, kind)
 
     @classmethod
+    def build_gpu(cls, vertices, indices, stream=None) -> "Scene":
+        """CWBVH built on the device (rq_build_scene_gpu) from CUDA tensors
+        vertices (nv, 3) float32 and indices (nt, 3) int32."""
+        h = C.c_void_p()
+        check(lib.rq_build_scene_gpu(_ptr(vertices), _rows(vertices, 3, "vertices"), _ptr(indices),
+                                     _rows(indices, 3, "indices"), C.byref(h), _stream(stream)),
+              "rq_build_scene_gpu")
+        return cls(h, CWBVH)
+
+    def download(self):
+        """Host copies (nodes (n, 4) float32, woop (m, 4) float32, prim_index) of the device buffers."""
+        import torch
+        n, w, p = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib.rq_scene_device_buffers(self._h, C.byref(n), C.byref(w), C.byref(p)), "rq_scene_device_buffers")
+        nn, nw, npi = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib.rq_scene_sizes(self._h, C.byref(nn), C.byref(nw), C.byref(npi)), "rq_scene_sizes")
+        out = []
+        for ptr, count, width, dt in ((n, nn.value, 4, torch.float32), (w, nw.value, 4, torch.float32),
+                                      (p, npi.value, 1, torch.int32)):
+            t = torch.empty((count, width) if width > 1 else (count,), dtype=dt, device="cuda")
+            if count:
+                check(lib.rq_device_copy(t.data_ptr(), ptr, count * width * 4), "rq_device_copy")
+            out.append(t.cpu().numpy())
+        return tuple(out)
+
+    @classmethod
     def from_device(cls, kind: int, nodes, woop, prim_index=None) -> "Scene":
         """Borrow device tensors (kept alive by the Scene object)."""
         h = C.c_void_p()

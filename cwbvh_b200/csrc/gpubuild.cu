@@ -1,0 +1,562 @@
+// CWBVH built on the GPU from device-resident triangles, for scenes that must
+// be ready quickly (a new scene admitted into a server) rather than traced
+// at the best speed: a linear BVH (Morton-ordered triangles, Karras's radix
+// tree, bottom-up boxes) collapsed top-down into 8-wide nodes written
+// directly in the CWBVH node format, with Woop rows and the primitive map,
+// all on one stream.
+//
+//  1. centroid bounds (reduction), Morton code of each centroid above the
+//     triangle number (unique 64-bit keys: ceil(log2 n) index bits, the rest,
+//     up to 21 per axis, for the code), radix sort;
+//  2. internal node i of the binary radix tree over the sorted keys: its key
+//     range and split from the longest common prefixes (Karras, "Maximizing
+//     Parallelism in the Construction of BVHs, Octrees, and k-d Trees",
+//     HPG 2012), parent links;
+//  3. boxes and triangle counts bottom-up: each leaf walks to the root and
+//     the second thread to reach a node completes it (one atomic per node);
+//  4. level by level from the root: a binary node that becomes an 8-wide
+//     node opens its largest child until it has 8 children; children with at
+//     most 3 triangles become leaves, the others 8-wide nodes of the next
+//     level.  Slots are assigned by the same octant rule as the host
+//     converter, boxes quantized the same way, inner children get one
+//     contiguous block and leaf triangles one contiguous run per node.
+//
+// The tree is a valid CWBVH for every trace kernel; it is not the host
+// builder's (no SAH), so traversal is slower and the bytes differ.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+
+#include "runtime.h"
+
+namespace rq {
+namespace {
+
+struct BNode {
+    int32_t left, right;  // >= 0: internal node, < 0: leaf ~(sorted position)
+    int32_t parent;       // -1 at the root
+    int32_t count;        // triangles below
+    float lo[3], hi[3];
+};
+
+__device__ inline unsigned f2ord(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ inline float ord2f(unsigned u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u); }
+
+__device__ inline float3 vtx(const float* v, int32_t k) {
+    const int64_t o = 3 * (int64_t)k;
+    return make_float3(v[o], v[o + 1], v[o + 2]);
+}
+
+__device__ inline void tri_box(const float* v, const int32_t* idx, int64_t t, float lo[3], float hi[3]) {
+    const float3 a = vtx(v, idx[3 * t]), b = vtx(v, idx[3 * t + 1]), c = vtx(v, idx[3 * t + 2]);
+    lo[0] = fminf(a.x, fminf(b.x, c.x)); hi[0] = fmaxf(a.x, fmaxf(b.x, c.x));
+    lo[1] = fminf(a.y, fminf(b.y, c.y)); hi[1] = fmaxf(a.y, fmaxf(b.y, c.y));
+    lo[2] = fminf(a.z, fminf(b.z, c.z)); hi[2] = fmaxf(a.z, fmaxf(b.z, c.z));
+}
+
+// Sets *bad when an index is outside [0, nv): nothing else reads vertices
+// through indices that have not passed this check.
+__global__ void check_indices_kernel(const int32_t* idx, int64_t n3, int64_t nv, unsigned* bad) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n3; q += (int64_t)gridDim.x * blockDim.x)
+        if (idx[q] < 0 || (int64_t)idx[q] >= nv) atomicOr(bad, 1u);
+}
+
+// Centroid bounds as order-preserving unsigned min / max (6 words).
+__global__ void centroid_bounds_kernel(const float* v, const int32_t* idx, int64_t n, unsigned* ob) {
+    unsigned mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        float lo[3], hi[3];
+        tri_box(v, idx, t, lo, hi);
+        for (int a = 0; a < 3; ++a) {
+            const unsigned c = f2ord(0.5f * (lo[a] + hi[a]));
+            mn[a] = min(mn[a], c);
+            mx[a] = max(mx[a], c);
+        }
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[a] = min(mn[a], __shfl_xor_sync(0xFFFFFFFFu, mn[a], o));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xFFFFFFFFu, mx[a], o));
+        }
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(ob + a, mn[a]);
+            atomicMax(ob + 3 + a, mx[a]);
+        }
+}
+
+// Spreads the low 21 bits of x to every third bit.
+__device__ inline uint64_t spread3(uint64_t x) {
+    x &= 0x1FFFFFull;
+    x = (x | (x << 32)) & 0x001F00000000FFFFull;
+    x = (x | (x << 16)) & 0x001F0000FF0000FFull;
+    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+// key = Morton code of the centroid (`axis_bits` per axis) above the
+// triangle number (`idx_bits`): unique, and as fine a grid as 64 bits allow.
+__global__ void morton_kernel(const float* v, const int32_t* idx, int64_t n, const unsigned* ob, int axis_bits,
+                              int idx_bits, uint64_t* keys) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    float lo[3], hi[3];
+    tri_box(v, idx, t, lo, hi);
+    const float cells = (float)(1u << axis_bits);
+    uint64_t q[3];
+    for (int a = 0; a < 3; ++a) {
+        const float b0 = ord2f(ob[a]), b1 = ord2f(ob[3 + a]);
+        const float ext = b1 - b0;
+        float f = ext > 0.f ? (0.5f * (lo[a] + hi[a]) - b0) / ext : 0.f;
+        f = fminf(fmaxf(f, 0.f), 1.f);
+        q[a] = min((uint64_t)((1u << axis_bits) - 1), (uint64_t)(f * cells));
+    }
+    const uint64_t m = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+    keys[t] = (m << idx_bits) | (uint64_t)t;
+}
+
+__device__ inline int delta(const uint64_t* k, int64_t n, int64_t i, int64_t j) {
+    if (j < 0 || j >= n) return -1;
+    return __clzll((long long)(k[i] ^ k[j]));
+}
+
+// Internal node i of the radix tree (Karras 2012, section 4).
+__global__ void radix_tree_kernel(const uint64_t* k, int64_t n, BNode* nodes, int32_t* leaf_parent) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int d = delta(k, n, i, i + 1) - delta(k, n, i, i - 1) >= 0 ? 1 : -1;
+    const int dmin = delta(k, n, i, i - d);
+    int64_t lmax = 2;
+    while (delta(k, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int64_t l = 0;
+    for (int64_t t = lmax / 2; t >= 1; t /= 2)
+        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int64_t j = i + l * d;
+    const int dnode = delta(k, n, i, j);
+    int64_t s = 0;
+    for (int64_t div = 2;; div *= 2) {
+        const int64_t t = (l + div - 1) / div;
+        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+    }
+    const int64_t gamma = i + s * d + min(d, 0);
+    const int64_t lo = min(i, j), hi = max(i, j);
+    BNode& nd = nodes[i];
+    nd.left = lo == gamma ? ~(int32_t)gamma : (int32_t)gamma;
+    nd.right = hi == gamma + 1 ? ~(int32_t)(gamma + 1) : (int32_t)(gamma + 1);
+    if (nd.left >= 0) nodes[nd.left].parent = (int32_t)i;
+    else leaf_parent[gamma] = (int32_t)i;
+    if (nd.right >= 0) nodes[nd.right].parent = (int32_t)i;
+    else leaf_parent[gamma + 1] = (int32_t)i;
+    if (i == 0) nd.parent = -1;
+}
+
+// The triangle of a sorted key: its low idx_bits bits (idx_mask).
+__device__ inline int64_t key_tri(const uint64_t* k, int64_t pos, uint64_t idx_mask) {
+    return (int64_t)(k[pos] & idx_mask);
+}
+
+__device__ inline void child_box(const BNode* nodes, const uint64_t* k, uint64_t idx_mask, const float* v,
+                                 const int32_t* idx, int32_t code, float lo[3], float hi[3], int32_t& count) {
+    if (code >= 0) {
+        const volatile BNode& c = nodes[code];
+        for (int a = 0; a < 3; ++a) { lo[a] = c.lo[a]; hi[a] = c.hi[a]; }
+        count = c.count;
+    } else {
+        tri_box(v, idx, key_tri(k, ~code, idx_mask), lo, hi);
+        count = 1;
+    }
+}
+
+// Boxes and counts bottom-up: the second of a node's two children to arrive
+// completes it and goes on to the parent.
+__global__ void boxes_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, const float* v, const int32_t* idx,
+                             BNode* nodes, const int32_t* leaf_parent, int32_t* arrivals) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int32_t node = leaf_parent[p];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;  // the sibling finishes this node
+        __threadfence();
+        float l0[3], h0[3], l1[3], h1[3];
+        int32_t c0, c1;
+        child_box(nodes, k, idx_mask, v, idx, nodes[node].left, l0, h0, c0);
+        child_box(nodes, k, idx_mask, v, idx, nodes[node].right, l1, h1, c1);
+        volatile BNode& nd = nodes[node];
+        for (int a = 0; a < 3; ++a) {
+            nd.lo[a] = fminf(l0[a], l1[a]);
+            nd.hi[a] = fmaxf(h0[a], h1[a]);
+        }
+        nd.count = c0 + c1;
+        node = nodes[node].parent;
+    }
+}
+
+// ---- Woop rows (the host woopify, with every rounding explicit so that the
+// device gives the host's values for the same triangle).
+__device__ void woopify_dev(float3 v0, float3 v1, float3 v2, float4* out) {
+    const float3 e0 = make_float3(__fsub_rn(v0.x, v2.x), __fsub_rn(v0.y, v2.y), __fsub_rn(v0.z, v2.z));
+    const float3 e1 = make_float3(__fsub_rn(v1.x, v2.x), __fsub_rn(v1.y, v2.y), __fsub_rn(v1.z, v2.z));
+    const float3 nn = make_float3(__fsub_rn(__fmul_rn(e0.y, e1.z), __fmul_rn(e0.z, e1.y)),
+                                  __fsub_rn(__fmul_rn(e0.z, e1.x), __fmul_rn(e0.x, e1.z)),
+                                  __fsub_rn(__fmul_rn(e0.x, e1.y), __fmul_rn(e0.y, e1.x)));
+    const double a[3][3] = {{e0.x, e1.x, nn.x}, {e0.y, e1.y, nn.y}, {e0.z, e1.z, nn.z}};
+    const double t[3] = {v2.x, v2.y, v2.z};
+    auto m2 = [](double p, double q, double r, double s) { return __dsub_rn(__dmul_rn(p, q), __dmul_rn(r, s)); };
+    double c[3][3];
+    c[0][0] = m2(a[1][1], a[2][2], a[1][2], a[2][1]);
+    c[0][1] = m2(a[0][2], a[2][1], a[0][1], a[2][2]);
+    c[0][2] = m2(a[0][1], a[1][2], a[0][2], a[1][1]);
+    c[1][0] = m2(a[1][2], a[2][0], a[1][0], a[2][2]);
+    c[1][1] = m2(a[0][0], a[2][2], a[0][2], a[2][0]);
+    c[1][2] = m2(a[0][2], a[1][0], a[0][0], a[1][2]);
+    c[2][0] = m2(a[1][0], a[2][1], a[1][1], a[2][0]);
+    c[2][1] = m2(a[0][1], a[2][0], a[0][0], a[2][1]);
+    c[2][2] = m2(a[0][0], a[1][1], a[0][1], a[1][0]);
+    const double det = __dadd_rn(__dadd_rn(__dmul_rn(a[0][0], c[0][0]), __dmul_rn(a[0][1], c[1][0])),
+                                 __dmul_rn(a[0][2], c[2][0]));
+    if (det == 0.0 || !isfinite(det)) {
+        out[0] = out[1] = out[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const double rdet = __ddiv_rn(1.0, det);
+    double inv[3][4];
+    for (int r = 0; r < 3; ++r) {
+        for (int q = 0; q < 3; ++q) inv[r][q] = __dmul_rn(c[r][q], rdet);
+        inv[r][3] = -__dadd_rn(__dadd_rn(__dmul_rn(inv[r][0], t[0]), __dmul_rn(inv[r][1], t[1])),
+                               __dmul_rn(inv[r][2], t[2]));
+    }
+    float x0 = (float)inv[2][0];
+    if (x0 == 0.0f) x0 = 0.0f;  // -0.0f would read as a BVH2 leaf terminator
+    out[0] = make_float4(x0, (float)inv[2][1], (float)inv[2][2], (float)(-inv[2][3]));
+    out[1] = make_float4((float)inv[0][0], (float)inv[0][1], (float)inv[0][2], (float)inv[0][3]);
+    out[2] = make_float4((float)inv[1][0], (float)inv[1][1], (float)inv[1][2], (float)inv[1][3]);
+}
+
+struct Item {
+    int32_t code;  // binary node (>= 0) or a single-triangle root (< 0)
+    int32_t addr;  // 8-wide node index
+};
+
+struct Ctr {
+    unsigned long long nodes;  // 8-wide nodes allocated
+    unsigned long long tris;   // triangle slots allocated
+    unsigned long long next;   // items of the next level
+    unsigned int error;
+};
+
+__device__ inline float area(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Expands the binary nodes of one level into 8-wide nodes.
+__global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, int64_t next_cap, const BNode* nodes,
+                              const uint64_t* k, uint64_t idx_mask, const float* v, const int32_t* idx,
+                              float4* out_nodes,
+                              int64_t node_cap, float4* woop, int32_t* prim, int64_t tri_cap, Ctr* ctr) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_items) return;
+    const Item it = items[w];
+    int32_t code[8];
+    float clo[8][3], chi[8][3];
+    int32_t cnt[8];
+    int m = 0;
+    if (it.code < 0) {  // one triangle: the root holds one leaf
+        code[0] = it.code;
+        child_box(nodes, k, idx_mask, v, idx, it.code, clo[0], chi[0], cnt[0]);
+        m = 1;
+    } else {
+        const BNode& b = nodes[it.code];
+        code[0] = b.left;
+        code[1] = b.right;
+        child_box(nodes, k, idx_mask, v, idx, b.left, clo[0], chi[0], cnt[0]);
+        child_box(nodes, k, idx_mask, v, idx, b.right, clo[1], chi[1], cnt[1]);
+        m = 2;
+        // open the largest child that would become an 8-wide node, while slots remain
+        while (m < 8) {
+            int best = -1;
+            float ba = -1.f;
+            for (int c = 0; c < m; ++c)
+                if (code[c] >= 0 && cnt[c] > 3 && area(clo[c], chi[c]) > ba) { ba = area(clo[c], chi[c]); best = c; }
+            if (best < 0) break;
+            const BNode& o = nodes[code[best]];
+            const int32_t l = o.left, r = o.right;
+            code[best] = l;
+            child_box(nodes, k, idx_mask, v, idx, l, clo[best], chi[best], cnt[best]);
+            code[m] = r;
+            child_box(nodes, k, idx_mask, v, idx, r, clo[m], chi[m], cnt[m]);
+            ++m;
+        }
+    }
+    // node box
+    float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int c = 0; c < m; ++c)
+        for (int a = 0; a < 3; ++a) { lo[a] = fminf(lo[a], clo[c][a]); hi[a] = fmaxf(hi[a], chi[c][a]); }
+    // octant slots: cheapest (slot, child) pairs first, as the host converter
+    float nc[3];
+    for (int a = 0; a < 3; ++a) nc[a] = (lo[a] + hi[a]) * 0.5f;
+    int slot_of[8], child_in[8];
+    bool slot_free[8];
+    for (int s = 0; s < 8; ++s) { slot_of[s] = -1; slot_free[s] = true; child_in[s] = -1; }
+    for (;;) {
+        float best = FLT_MAX;
+        int bs = -1, bc = -1;
+        for (int s = 0; s < 8; ++s) {
+            if (!slot_free[s]) continue;
+            const float dx = (s & 4) ? -1.f : 1.f, dy = (s & 2) ? -1.f : 1.f, dz = (s & 1) ? -1.f : 1.f;
+            for (int c = 0; c < m; ++c) {
+                if (slot_of[c] >= 0) continue;
+                const float cx = __fsub_rn(__fmul_rn(__fadd_rn(clo[c][0], chi[c][0]), 0.5f), nc[0]);
+                const float cy = __fsub_rn(__fmul_rn(__fadd_rn(clo[c][1], chi[c][1]), 0.5f), nc[1]);
+                const float cz = __fsub_rn(__fmul_rn(__fadd_rn(clo[c][2], chi[c][2]), 0.5f), nc[2]);
+                const float cost = __fadd_rn(__fadd_rn(__fmul_rn(cx, dx), __fmul_rn(cy, dy)), __fmul_rn(cz, dz));
+                if (cost < best) { best = cost; bs = s; bc = c; }
+            }
+        }
+        if (bs < 0) break;
+        slot_free[bs] = false;
+        slot_of[bc] = bs;
+        child_in[bs] = bc;
+    }
+    // per-axis exponent, grown while a child's upper bound does not fit a byte
+    int e[3];
+    for (int a = 0; a < 3; ++a) {
+        const float r = ceilf(log2f((hi[a] - lo[a]) / 255.0f));
+        e[a] = isfinite(r) ? (int)fmaxf(-127.f, fminf(127.f, r)) : 0;
+        for (;;) {
+            const float scale = ldexpf(1.0f, e[a]);
+            bool fits = true;
+            for (int c = 0; c < m; ++c)
+                if ((int)ceilf((chi[c][a] - lo[a]) / scale) > 255) fits = false;
+            if (fits || e[a] >= 127) break;
+            ++e[a];
+        }
+    }
+    // allocations: inner children as one block, leaf triangles as one run
+    int n_inner = 0, n_tris = 0;
+    for (int c = 0; c < m; ++c) {
+        if (cnt[c] > 3) ++n_inner;
+        else n_tris += cnt[c];
+    }
+    const unsigned long long base = n_inner ? atomicAdd(&ctr->nodes, (unsigned long long)n_inner) : 0ull;
+    const unsigned long long tbase = n_tris ? atomicAdd(&ctr->tris, (unsigned long long)n_tris) : 0ull;
+    const unsigned long long qbase = n_inner ? atomicAdd(&ctr->next, (unsigned long long)n_inner) : 0ull;
+    if (base + n_inner > (unsigned long long)node_cap || tbase + n_tris > (unsigned long long)tri_cap ||
+        qbase + n_inner > (unsigned long long)next_cap) {
+        atomicOr(&ctr->error, 1u);
+        return;
+    }
+    float4 node[5];
+    for (int q = 0; q < 5; ++q) node[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned char* bytes = reinterpret_cast<unsigned char*>(node);
+    uint8_t imask = 0;
+    int inner = 0, leaf_tris = 0;
+    for (int s = 0; s < 8; ++s) {
+        const int c = child_in[s];
+        if (c < 0) continue;
+        for (int a = 0; a < 3; ++a) {
+            const float scale = ldexpf(1.0f, e[a]);
+            bytes[32 + s + 8 * a] = (uint8_t)(int)floorf((clo[c][a] - lo[a]) / scale);
+            bytes[32 + s + 8 * (3 + a)] = (uint8_t)(int)ceilf((chi[c][a] - lo[a]) / scale);
+        }
+        if (cnt[c] > 3) {
+            imask |= (uint8_t)(1u << s);
+            bytes[24 + s] = (uint8_t)((1u << 5) | (24u + s));
+            next[qbase + inner] = Item{code[c], (int32_t)(base + inner)};
+            ++inner;
+        } else {
+            const uint32_t unary = cnt[c] == 1 ? 1u : (cnt[c] == 2 ? 3u : 7u);
+            bytes[24 + s] = (uint8_t)((unary << 5) | ((uint32_t)leaf_tris & 31u));
+            // the child's triangles: a leaf, or a subtree of at most 3
+            int32_t st[4];
+            int sp = 0;
+            st[sp++] = code[c];
+            while (sp > 0) {
+                const int32_t x = st[--sp];
+                if (x < 0) {
+                    const int64_t tri = key_tri(k, ~x, idx_mask);
+                    const int64_t slot = (int64_t)tbase + leaf_tris;
+                    const int32_t* ti = idx + 3 * tri;
+                    woopify_dev(vtx(v, ti[0]), vtx(v, ti[1]), vtx(v, ti[2]), woop + 3 * slot);
+                    prim[3 * slot] = (int32_t)tri;
+                    prim[3 * slot + 1] = -1;
+                    prim[3 * slot + 2] = -1;
+                    ++leaf_tris;
+                } else {
+                    st[sp++] = nodes[x].right;
+                    st[sp++] = nodes[x].left;
+                }
+            }
+        }
+    }
+    float* nf = reinterpret_cast<float*>(bytes);
+    nf[0] = lo[0];
+    nf[1] = lo[1];
+    nf[2] = lo[2];
+    bytes[12] = (uint8_t)(int8_t)e[0];
+    bytes[13] = (uint8_t)(int8_t)e[1];
+    bytes[14] = (uint8_t)(int8_t)e[2];
+    bytes[15] = imask;
+    reinterpret_cast<int32_t*>(bytes)[4] = inner ? (int32_t)base : 0;
+    reinterpret_cast<int32_t*>(bytes)[5] = leaf_tris ? (int32_t)tbase : 0;
+    for (int q = 0; q < 5; ++q) out_nodes[(int64_t)it.addr * 5 + q] = node[q];
+}
+
+unsigned blocks_of(int64_t n, int b) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
+
+}  // namespace
+}  // namespace rq
+
+using namespace rq;
+
+extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt,
+                                        rq_scene_t* out, void* stream) {
+    if (!out || !vertices || !indices || nv <= 0 || nt <= 0 || nt > (int64_t)INT32_MAX / 4) return RQ_ERR_INVALID_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t n = nt;
+    // device scratch
+    uint64_t *keys = nullptr, *keys_sorted = nullptr;
+    BNode* bn = nullptr;
+    int32_t *leaf_parent = nullptr, *arrivals = nullptr;
+    unsigned* ob = nullptr;
+    Item *qa = nullptr, *qb = nullptr;
+    Ctr* ctr = nullptr;
+    void* cub_temp = nullptr;
+    float4 *nodes = nullptr, *woop = nullptr;
+    int32_t* prim = nullptr;
+    size_t cub_bytes = 0;
+    int idx_bits = 1;
+    while ((1ll << idx_bits) < n) ++idx_bits;
+    const uint64_t idx_mask = (1ull << idx_bits) - 1;
+    const int axis_bits = std::min(21, (64 - idx_bits) / 3);
+    const int end_bit = idx_bits + 3 * axis_bits;
+    rq_status st = RQ_OK;
+    auto ok = [&](cudaError_t e, const char* what) {
+        if (e != cudaSuccess && st == RQ_OK) st = cuda_fail(e, what);
+        return st == RQ_OK;
+    };
+    const int64_t node_cap = std::max<int64_t>(1, n);  // an 8-wide node per binary node at most
+    const int64_t q_cap = node_cap;
+    constexpr size_t kPad = 256;
+    if (ok(cudaMalloc(&keys, n * sizeof(uint64_t)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&keys_sorted, n * sizeof(uint64_t)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&bn, std::max<int64_t>(1, n - 1) * sizeof(BNode)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&leaf_parent, n * sizeof(int32_t)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&arrivals, std::max<int64_t>(1, n - 1) * sizeof(int32_t)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&ob, 6 * sizeof(unsigned)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&qa, q_cap * sizeof(Item)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&qb, q_cap * sizeof(Item)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&ctr, sizeof(Ctr)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&nodes, node_cap * 80 + kPad), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&woop, n * 48 + kPad), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&prim, n * 12), "rq_build_scene_gpu")) {
+        const unsigned init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+        ok(cudaMemcpyAsync(ob, init, sizeof(init), cudaMemcpyHostToDevice, s), "rq_build_scene_gpu");
+        ok(cudaMemsetAsync(nodes, 0, node_cap * 80 + kPad, s), "rq_build_scene_gpu");
+        ok(cudaMemsetAsync(woop, 0, n * 48 + kPad, s), "rq_build_scene_gpu");
+        ok(cudaMemsetAsync(arrivals, 0, std::max<int64_t>(1, n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
+        ok(cudaMemsetAsync(ctr, 0, sizeof(Ctr), s), "rq_build_scene_gpu");
+    }
+    if (st == RQ_OK) {
+        // indices first: the kernels below read vertices through them
+        unsigned bad = 0;
+        ok(cudaMemsetAsync(&ctr->error, 0, sizeof(unsigned), s), "rq_build_scene_gpu");
+        check_indices_kernel<<<std::min<unsigned>(blocks_of(3 * n, 256), 8 * 148), 256, 0, s>>>(indices, 3 * n, nv,
+                                                                                                 &ctr->error);
+        ok(cudaGetLastError(), "rq_build_scene_gpu");
+        ok(cudaMemcpyAsync(&bad, &ctr->error, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "rq_build_scene_gpu");
+        ok(cudaStreamSynchronize(s), "rq_build_scene_gpu");
+        if (st == RQ_OK && bad) st = RQ_ERR_INVALID_ARG;
+    }
+    if (st == RQ_OK) {
+        centroid_bounds_kernel<<<std::min<unsigned>(blocks_of(n, 256), 4 * 148), 256, 0, s>>>(vertices, indices, n, ob);
+        morton_kernel<<<blocks_of(n, 256), 256, 0, s>>>(vertices, indices, n, ob, axis_bits, idx_bits, keys);
+        ok(cudaGetLastError(), "rq_build_scene_gpu");
+        ok(cub::DeviceRadixSort::SortKeys(nullptr, cub_bytes, keys, keys_sorted, (int)n, 0, end_bit, s),
+           "rq_build_scene_gpu");
+        ok(cudaMalloc(&cub_temp, std::max<size_t>(cub_bytes, 1)), "rq_build_scene_gpu");
+        ok(cub::DeviceRadixSort::SortKeys(cub_temp, cub_bytes, keys, keys_sorted, (int)n, 0, end_bit, s),
+           "rq_build_scene_gpu");
+    }
+    int64_t levels = 0, n_nodes = 1;
+    if (st == RQ_OK && n > 1) {
+        radix_tree_kernel<<<blocks_of(n - 1, 256), 256, 0, s>>>(keys_sorted, n, bn, leaf_parent);
+        boxes_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn, leaf_parent,
+                                                       arrivals);
+        ok(cudaGetLastError(), "rq_build_scene_gpu");
+    }
+    if (st == RQ_OK) {
+        // level 0: the root (binary node 0, or the single triangle)
+        const Item root{n > 1 ? 0 : ~0, 0};
+        const Ctr c0{1ull, 0ull, 0ull, 0u};
+        ok(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, s), "rq_build_scene_gpu");
+        ok(cudaMemcpyAsync(ctr, &c0, sizeof(c0), cudaMemcpyHostToDevice, s), "rq_build_scene_gpu");
+        int64_t n_items = 1;
+        while (st == RQ_OK && n_items > 0) {
+            expand_kernel<<<blocks_of(n_items, 128), 128, 0, s>>>(qa, n_items, qb, q_cap, bn, keys_sorted, idx_mask,
+                                                                  vertices, indices, nodes, node_cap, woop, prim, n,
+                                                                  ctr);
+            ok(cudaGetLastError(), "rq_build_scene_gpu");
+            Ctr c{};
+            ok(cudaMemcpyAsync(&c, ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, s), "rq_build_scene_gpu");
+            ok(cudaStreamSynchronize(s), "rq_build_scene_gpu");
+            if (st != RQ_OK) break;
+            if (c.error) {
+                st = RQ_ERR_BAD_SCENE;  // capacity exceeded: cannot happen for a valid radix tree
+                break;
+            }
+            n_items = (int64_t)c.next;
+            n_nodes = (int64_t)c.nodes;
+            std::swap(qa, qb);
+            ok(cudaMemsetAsync(&ctr->next, 0, sizeof(unsigned long long), s), "rq_build_scene_gpu");
+            if (++levels > 4096) st = RQ_ERR_BAD_SCENE;
+        }
+    }
+    float root[20] = {};
+    if (st == RQ_OK) ok(cudaMemcpy(root, nodes, sizeof(root), cudaMemcpyDeviceToHost), "rq_build_scene_gpu");
+    cudaFree(keys);
+    cudaFree(keys_sorted);
+    cudaFree(bn);
+    cudaFree(leaf_parent);
+    cudaFree(arrivals);
+    cudaFree(ob);
+    cudaFree(qa);
+    cudaFree(qb);
+    cudaFree(ctr);
+    cudaFree(cub_temp);
+    if (st != RQ_OK) {
+        cudaFree(nodes);
+        cudaFree(woop);
+        cudaFree(prim);
+        return st;
+    }
+    rq_scene* sc = new rq_scene();
+    sc->kind = RQ_BVH_CWBVH;
+    cudaGetDevice(&sc->device);
+    sc->nodes = nodes;
+    sc->woop = woop;
+    sc->prim_index = prim;
+    sc->node_f4 = n_nodes * 5;
+    sc->woop_f4 = n * 3;
+    sc->prim_count = n * 3;
+    sc->owned = true;
+    uint32_t ew;
+    std::memcpy(&ew, &root[3], 4);
+    for (int a = 0; a < 3; ++a) {
+        const int e = (int)(int8_t)((ew >> (8 * a)) & 0xFFu);
+        sc->lo[a] = root[a];
+        sc->hi[a] = root[a] + 255.0f * std::ldexp(1.0f, e);
+    }
+    *out = sc;
+    return RQ_OK;
+}

@@ -311,6 +311,14 @@ rq_status rq_scene_device_buffers(rq_scene_t scene, const void** nodes, const vo
     return RQ_OK;
 }
 
+rq_status rq_scene_sizes(rq_scene_t scene, int64_t* node_float4s, int64_t* woop_float4s, int64_t* prim_index_count) {
+    if (!scene) return RQ_ERR_INVALID_ARG;
+    if (node_float4s) *node_float4s = scene->node_f4;
+    if (woop_float4s) *woop_float4s = scene->woop_f4;
+    if (prim_index_count) *prim_index_count = scene->prim_count;
+    return RQ_OK;
+}
+
 int64_t rq_scene_bytes(rq_scene_t scene) {
     if (!scene) return 0;
     return scene->node_f4 * 16 + scene->woop_f4 * 16 + scene->prim_count * 4;

@@ -153,6 +153,9 @@ rq_status rq_scene_from_host_bvh(rq_host_bvh_t bvh, rq_scene_t* out);
 rq_status rq_scene_destroy(rq_scene_t scene);
 rq_status rq_scene_device_buffers(rq_scene_t scene, const void** nodes, const void** woop,
                                   const int32_t** prim_index);
+/* Buffer lengths of a scene: node and Woop float4s, primitive-map entries. */
+rq_status rq_scene_sizes(rq_scene_t scene, int64_t* node_float4s, int64_t* woop_float4s,
+                         int64_t* prim_index_count);
 int64_t rq_scene_bytes(rq_scene_t scene);
 
 /* ---------------------------------------------------------------- contexts */
@@ -460,6 +463,20 @@ rq_status rq_rtOccludedBVH2(void* rays, void* hits, int ray_count);
  * returned (rq_GenerateAORaysUniform). */
 rq_status rq_device_copy(void* dst, const void* src, int64_t bytes);
 rq_status rq_device_free(void* p);
+
+/* ------------------------------------------------------------ GPU build */
+/*
+ * A CWBVH scene built on the device from device-resident vertices (3*nv
+ * floats) and indices (3*nt ints) on `stream`: Morton-ordered linear BVH
+ * (Karras's radix tree), bottom-up boxes, top-down collapse to 8-wide nodes
+ * written in the CWBVH format with Woop rows and the primitive map.  Much
+ * faster to build than rq_build_bvh, slower to trace (no SAH); the scene
+ * owns its buffers (rq_scene_destroy).  No reference counterpart (the
+ * reference builds on the host with Embree).  Indices outside [0, nv) give
+ * RQ_ERR_INVALID_ARG.  Synchronises `stream` once per tree level.
+ */
+rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt,
+                             rq_scene_t* out, void* stream);
 
 /* ------------------------------------------------------- instancing (TLAS) */
 /*
