@@ -1100,21 +1100,26 @@ def run_large(args, world, rank, dist):
         return
     ms_plain = time_steps(lambda: rq.trace(ctx, sc, rays, hits, rq.ANY, stream=stream), args.steps, warmup, stream,
                           dist)
-    # the same mesh built on the GPU (linear BVH collapsed to CWBVH): build time and trace speed
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    gsc = rq.Scene.build_gpu(v, i, stream=stream)
-    torch.cuda.synchronize()
-    t_gpu_build = time.perf_counter() - t0
-    del v, i
+    # the same mesh built on the GPU (linear BVH, then 0 or 2 treelet passes, collapsed to CWBVH)
+    gpu_trees = {}
     with torch.cuda.stream(stream):
         ghits = torch.empty((n, 4), device="cuda")
-    ms_gpu_tree = time_steps(lambda: rq.trace(ctx, gsc, rays, ghits, rq.ANY, stream=stream), args.steps, warmup,
-                             stream, dist)
-    ctx.check(stream)
-    torch.cuda.synchronize()
-    gpu_same = float(((ghits[:, 1].view(torch.int32) != -1) == (hits[:, 1].view(torch.int32) != -1)).float().mean())
-    del ghits, gsc
+    for passes in (0, 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gsc = rq.Scene.build_gpu(v, i, optimize_passes=passes, stream=stream)
+        torch.cuda.synchronize()
+        t_gpu_build = time.perf_counter() - t0
+        ms_gpu_tree = time_steps(lambda: rq.trace(ctx, gsc, rays, ghits, rq.ANY, stream=stream), args.steps, warmup,
+                                 stream, dist)
+        ctx.check(stream)
+        torch.cuda.synchronize()
+        same = float(((ghits[:, 1].view(torch.int32) != -1) == (hits[:, 1].view(torch.int32) != -1)).float().mean())
+        gpu_trees[f"treelet_passes_{passes}"] = {"build_s": round(t_gpu_build, 3),
+                                                 "mrays_per_s": round(n / (ms_gpu_tree * 1e-3) / 1e6, 2),
+                                                 "occlusion_same_frac": round(same, 6)}
+        del gsc
+    del v, i, ghits
     with torch.cuda.stream(stream):
         occl = torch.zeros(n // spp, dtype=torch.int32, device="cuda")
 
@@ -1145,10 +1150,9 @@ def run_large(args, world, rank, dist):
                    "fused_ao_counts": dict(_pass("fused", n, ms_fused),
                                            what="rq_trace_ao: per-surfel occluded counts in the trace epilogue, "
                                                 "no hit buffer (memset of the counts included)")},
-        "gpu_built_tree": {"build_s": round(t_gpu_build, 3), "host_build_s": round(t_host_build, 2),
-                           "mrays_per_s": round(n / (ms_gpu_tree * 1e-3) / 1e6, 2),
-                           "occlusion_same_frac": round(gpu_same, 6),
-                           "what": "rq_build_scene_gpu: Morton-ordered linear BVH collapsed to CWBVH on the device"},
+        "gpu_built_tree": dict(gpu_trees, host_build_s=round(t_host_build, 2),
+                               what="rq_build_scene_gpu: Morton-ordered linear BVH, treelet restructuring passes, "
+                                    "collapsed to CWBVH on the device"),
         "sorted_occlusion_identical": same, "fused_counts_identical": fused_same,
         "ao_occluded_fraction": round(occ, 4),
         "triangles": int(I.shape[0]), "scene_bytes": int(hb.nodes.nbytes + hb.woop.nbytes),

@@ -283,12 +283,12 @@ class Scene:
         return cls(h, kind)
 
     @classmethod
-    def build_gpu(cls, vertices, indices, stream=None) -> "Scene":
+    def build_gpu(cls, vertices, indices, optimize_passes: int = 2, stream=None) -> "Scene":
         """CWBVH built on the device (rq_build_scene_gpu) from CUDA tensors
         vertices (nv, 3) float32 and indices (nt, 3) int32."""
         h = C.c_void_p()
         check(lib.rq_build_scene_gpu(_ptr(vertices), _rows(vertices, 3, "vertices"), _ptr(indices),
-                                     _rows(indices, 3, "indices"), C.byref(h), _stream(stream)),
+                                     _rows(indices, 3, "indices"), optimize_passes, C.byref(h), _stream(stream)),
               "rq_build_scene_gpu")
         return cls(h, CWBVH)
 

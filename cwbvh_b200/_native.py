@@ -160,5 +160,5 @@ _sig("rq_tlas_buffers", C.c_int, vp, P(vp), P(i64), P(vp), P(i64), P(vp))
 _sig("rq_trace_instanced", C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, P(Launch), vp)
 _sig("rq_tlas_build_host", C.c_int, vp, C.c_int, vp, vp, i64, P(vp))
 _sig("rq_server_submit_bake", C.c_int, vp, i32, vp, vp, vp, i64, C.c_int, u64, f32, f32, f32, vp, P(u64))
-_sig("rq_build_scene_gpu", C.c_int, vp, i64, vp, i64, P(vp), vp)
+_sig("rq_build_scene_gpu", C.c_int, vp, i64, vp, i64, C.c_int, P(vp), vp)
 _sig("rq_scene_sizes", C.c_int, vp, P(i64), P(i64), P(i64))

@@ -40,7 +40,12 @@ struct BNode {
     int32_t parent;       // -1 at the root
     int32_t count;        // triangles below
     float lo[3], hi[3];
+    float cost;           // SAH cost of the subtree
 };
+
+// SAH weights of the treelet restructuring (Karras and Aila 2013).
+constexpr float kCt = 1.2f;  // per node
+constexpr float kCi = 1.0f;  // per triangle
 
 __device__ inline unsigned f2ord(float f) {
     const unsigned u = __float_as_uint(f);
@@ -164,15 +169,23 @@ __device__ inline int64_t key_tri(const uint64_t* k, int64_t pos, uint64_t idx_m
     return (int64_t)(k[pos] & idx_mask);
 }
 
+__device__ inline float half_area(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
 __device__ inline void child_box(const BNode* nodes, const uint64_t* k, uint64_t idx_mask, const float* v,
-                                 const int32_t* idx, int32_t code, float lo[3], float hi[3], int32_t& count) {
+                                 const int32_t* idx, int32_t code, float lo[3], float hi[3], int32_t& count,
+                                 float* cost = nullptr) {
     if (code >= 0) {
         const volatile BNode& c = nodes[code];
         for (int a = 0; a < 3; ++a) { lo[a] = c.lo[a]; hi[a] = c.hi[a]; }
         count = c.count;
+        if (cost) *cost = c.cost;
     } else {
         tri_box(v, idx, key_tri(k, ~code, idx_mask), lo, hi);
         count = 1;
+        if (cost) *cost = kCi * half_area(lo, hi);
     }
 }
 
@@ -187,17 +200,172 @@ __global__ void boxes_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, co
         __threadfence();
         if (atomicAdd(&arrivals[node], 1) == 0) return;  // the sibling finishes this node
         __threadfence();
-        float l0[3], h0[3], l1[3], h1[3];
+        float l0[3], h0[3], l1[3], h1[3], k0, k1;
         int32_t c0, c1;
-        child_box(nodes, k, idx_mask, v, idx, nodes[node].left, l0, h0, c0);
-        child_box(nodes, k, idx_mask, v, idx, nodes[node].right, l1, h1, c1);
+        child_box(nodes, k, idx_mask, v, idx, nodes[node].left, l0, h0, c0, &k0);
+        child_box(nodes, k, idx_mask, v, idx, nodes[node].right, l1, h1, c1, &k1);
         volatile BNode& nd = nodes[node];
+        float lo[3], hi[3];
         for (int a = 0; a < 3; ++a) {
-            nd.lo[a] = fminf(l0[a], l1[a]);
-            nd.hi[a] = fmaxf(h0[a], h1[a]);
+            lo[a] = fminf(l0[a], l1[a]);
+            hi[a] = fmaxf(h0[a], h1[a]);
+            nd.lo[a] = lo[a];
+            nd.hi[a] = hi[a];
         }
         nd.count = c0 + c1;
+        nd.cost = kCt * half_area(lo, hi) + k0 + k1;
         node = nodes[node].parent;
+    }
+}
+
+// ---- Treelet restructuring (Karras and Aila, "Fast Parallel Construction of
+// High-Quality Bounding Volume Hierarchies", HPG 2013): bottom-up again, each
+// node with at least `min_count` triangles forms a treelet by expanding its
+// largest-area leaf until it has 7 leaves, finds the SAH-optimal binary tree
+// over those leaves by dynamic programming over the 127 leaf subsets, and
+// rebuilds the treelet with it (reusing its 6 internal nodes) when cheaper.
+// Treelets of different nodes being restructured at once are disjoint: a node
+// is processed only when both its children are final.
+constexpr int kTreeletLeaves = 7;
+
+// Node fields other threads of the same launch may have rewritten are read
+// from L2 (ld.cg), never from a possibly stale L1 line.
+__device__ inline int32_t ld_left(const BNode* nodes, int32_t x) { return __ldcg(&nodes[x].left); }
+__device__ inline int32_t ld_right(const BNode* nodes, int32_t x) { return __ldcg(&nodes[x].right); }
+__device__ inline int32_t ld_parent(const BNode* nodes, int32_t x) { return __ldcg(&nodes[x].parent); }
+
+__device__ void restructure(BNode* nodes, const uint64_t* k, uint64_t idx_mask, const float* v, const int32_t* idx,
+                            int32_t* leaf_parent, int32_t root) {
+    int32_t inner[kTreeletLeaves - 1], leaf[kTreeletLeaves];
+    float larea[kTreeletLeaves];
+    int n_in = 1, n_leaf = 2;
+    inner[0] = root;
+    leaf[0] = ld_left(nodes, root);
+    leaf[1] = ld_right(nodes, root);
+    float llo[kTreeletLeaves][3], lhi[kTreeletLeaves][3], lcost[kTreeletLeaves];
+    int32_t lcnt[kTreeletLeaves];
+    for (int q = 0; q < 2; ++q) {
+        child_box(nodes, k, idx_mask, v, idx, leaf[q], llo[q], lhi[q], lcnt[q], &lcost[q]);
+        larea[q] = half_area(llo[q], lhi[q]);
+    }
+    while (n_leaf < kTreeletLeaves) {
+        int best = -1;
+        float ba = -1.f;
+        for (int q = 0; q < n_leaf; ++q)
+            if (leaf[q] >= 0 && larea[q] > ba) { ba = larea[q]; best = q; }
+        if (best < 0) break;
+        const int32_t x = leaf[best];
+        inner[n_in++] = x;
+        const int32_t l = ld_left(nodes, x), r = ld_right(nodes, x);
+        leaf[best] = l;
+        child_box(nodes, k, idx_mask, v, idx, l, llo[best], lhi[best], lcnt[best], &lcost[best]);
+        larea[best] = half_area(llo[best], lhi[best]);
+        leaf[n_leaf] = r;
+        child_box(nodes, k, idx_mask, v, idx, r, llo[n_leaf], lhi[n_leaf], lcnt[n_leaf], &lcost[n_leaf]);
+        larea[n_leaf] = half_area(llo[n_leaf], lhi[n_leaf]);
+        ++n_leaf;
+    }
+    if (n_leaf < 3) return;
+    const int full = (1 << n_leaf) - 1;
+    float cost[1 << kTreeletLeaves], blo[1 << kTreeletLeaves][3], bhi[1 << kTreeletLeaves][3];
+    uint8_t part[1 << kTreeletLeaves];
+    for (int S = 1; S <= full; ++S) {
+        const int low = __ffs(S) - 1;
+        const int rest = S & (S - 1);
+        if (rest == 0) {
+            for (int a = 0; a < 3; ++a) { blo[S][a] = llo[low][a]; bhi[S][a] = lhi[low][a]; }
+            cost[S] = lcost[low];
+            part[S] = 0;
+            continue;
+        }
+        for (int a = 0; a < 3; ++a) {
+            blo[S][a] = fminf(blo[rest][a], llo[low][a]);
+            bhi[S][a] = fmaxf(bhi[rest][a], lhi[low][a]);
+        }
+        float best = FLT_MAX;
+        int bp = 0;
+        // partitions {P, S \ P} with the lowest leaf in P, P != S
+        for (int P = (S - 1) & S; P > 0; P = (P - 1) & S) {
+            if (!(P & (1 << low))) continue;
+            const float c = cost[P] + cost[S ^ P];
+            if (c < best) { best = c; bp = P; }
+        }
+        cost[S] = kCt * half_area(blo[S], bhi[S]) + best;
+        part[S] = (uint8_t)bp;
+    }
+    if (!(cost[full] < 0.999f * __ldcg(&nodes[root].cost))) return;
+    // every subset the new tree splits must have a split (finite costs); check
+    // before writing anything
+    {
+        int st[kTreeletLeaves], sp = 0;
+        st[sp++] = full;
+        while (sp > 0) {
+            const int S = st[--sp];
+            const int P = part[S];
+            if (P == 0 || (P & ~S) != 0 || P == S) return;
+            if (P & (P - 1)) st[sp++] = P;
+            if ((S ^ P) & ((S ^ P) - 1)) st[sp++] = S ^ P;
+            if (sp > kTreeletLeaves - 1) return;
+        }
+    }
+    // rebuild top-down: subset -> node, internal nodes taken from `inner`
+    int32_t st_set[kTreeletLeaves], st_node[kTreeletLeaves];
+    int sp = 0, used = 1;
+    st_set[sp] = full;
+    st_node[sp++] = root;
+    while (sp > 0) {
+        --sp;
+        const int S = st_set[sp];
+        const int32_t nd = st_node[sp];
+        const int P = part[S];
+        const int side[2] = {P, S ^ P};
+        int32_t code[2];
+        for (int c = 0; c < 2; ++c) {
+            const int T = side[c];
+            if ((T & (T - 1)) == 0) {  // one leaf of the treelet
+                code[c] = leaf[__ffs(T) - 1];
+                if (code[c] >= 0) nodes[code[c]].parent = nd;
+                else leaf_parent[~code[c]] = nd;
+            } else {
+                const int32_t ni = inner[used++];
+                code[c] = ni;
+                nodes[ni].parent = nd;
+                st_set[sp] = T;
+                st_node[sp++] = ni;
+            }
+        }
+        BNode& b = nodes[nd];
+        b.left = code[0];
+        b.right = code[1];
+        for (int a = 0; a < 3; ++a) { b.lo[a] = blo[S][a]; b.hi[a] = bhi[S][a]; }
+        int32_t cnt = 0;
+        for (int q = 0; q < n_leaf; ++q)
+            if (S & (1 << q)) cnt += lcnt[q];
+        b.count = cnt;
+        b.cost = cost[S];
+    }
+}
+
+__global__ void treelet_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, const float* v, const int32_t* idx,
+                               BNode* nodes, int32_t* leaf_parent, int32_t* arrivals, int min_count) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int32_t node = leaf_parent[p];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;
+        __threadfence();
+        // this node's cost from its (final) children, then its treelet
+        float l0[3], h0[3], l1[3], h1[3], k0, k1;
+        int32_t c0, c1;
+        child_box(nodes, k, idx_mask, v, idx, ld_left(nodes, node), l0, h0, c0, &k0);
+        child_box(nodes, k, idx_mask, v, idx, ld_right(nodes, node), l1, h1, c1, &k1);
+        volatile BNode& nd = nodes[node];
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) { lo[a] = fminf(l0[a], l1[a]); hi[a] = fmaxf(h0[a], h1[a]); }
+        nd.cost = kCt * half_area(lo, hi) + k0 + k1;
+        if (c0 + c1 >= min_count) restructure(nodes, k, idx_mask, v, idx, leaf_parent, node);
+        node = ld_parent(nodes, node);
     }
 }
 
@@ -383,6 +551,10 @@ __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, in
             st[sp++] = code[c];
             while (sp > 0) {
                 const int32_t x = st[--sp];
+                if (leaf_tris >= n_tris || (x >= 0 && sp + 2 > 4)) {  // counts disagree with the tree
+                    atomicOr(&ctr->error, 2u);
+                    return;
+                }
                 if (x < 0) {
                     const int64_t tri = key_tri(k, ~x, idx_mask);
                     const int64_t slot = (int64_t)tbase + leaf_tris;
@@ -420,7 +592,7 @@ unsigned blocks_of(int64_t n, int b) { return (unsigned)std::max<int64_t>(1, (n 
 using namespace rq;
 
 extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt,
-                                        rq_scene_t* out, void* stream) {
+                                        int optimize_passes, rq_scene_t* out, void* stream) {
     if (!out || !vertices || !indices || nv <= 0 || nt <= 0 || nt > (int64_t)INT32_MAX / 4) return RQ_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t n = nt;
@@ -494,6 +666,12 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
         boxes_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn, leaf_parent,
                                                        arrivals);
         ok(cudaGetLastError(), "rq_build_scene_gpu");
+        for (int pass = 0; pass < optimize_passes && st == RQ_OK; ++pass) {
+            ok(cudaMemsetAsync(arrivals, 0, (n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
+            treelet_kernel<<<blocks_of(n, 128), 128, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,
+                                                             leaf_parent, arrivals, kTreeletLeaves);
+            ok(cudaGetLastError(), "rq_build_scene_gpu");
+        }
     }
     if (st == RQ_OK) {
         // level 0: the root (binary node 0, or the single triangle)

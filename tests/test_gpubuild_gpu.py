@@ -17,12 +17,12 @@ def _device_mesh(V, I):
         torch.from_numpy(np.ascontiguousarray(I, np.int32)).cuda()
 
 
-@pytest.fixture(scope="module")
-def built(rq):
+@pytest.fixture(scope="module", params=[0, 2], ids=["linear", "treelets"])
+def built(rq, request):
     from cwbvh_b200 import workloads as W
     V, I = W.scene_of_size(3, 150_000)
     v, i = _device_mesh(V, I)
-    sc = rq.Scene.build_gpu(v, i)
+    sc = rq.Scene.build_gpu(v, i, optimize_passes=request.param)
     nodes, woop, prim = sc.download()
     return V, I, v, i, sc, nodes, woop, prim
 
