@@ -135,17 +135,8 @@ _sig("rq_GenerateAORaysUniform", vp, C.c_int, C.c_int, vp, vp, vp)
 _sig("rq_device_copy", C.c_int, vp, vp, i64)
 _sig("rq_device_free", C.c_int, vp)
 
-
-def check(status: int, where: str) -> None:
-    if status != RQ_OK:
-        raise RQError(status, where)
-
-
+# scene files, GPU build, sizes
 _sig("rq_convert_tree", C.c_int, i32, i64, vp, vp, i64, vp, vp, i64, vp, i32, vp, i64, vp, i64, P(vp))
-_sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)
-_sig("rq_camera_rays", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, f32, f32, vp, vp)
-_sig("rq_surfels_from_hits", C.c_int, vp, vp, vp, i64, vp, vp, vp, vp)
-_sig("rq_probe_l2_read", C.c_int, vp, i64, C.c_int, vp, vp)
 _sig("rq_load_mesh_dat", C.c_int, cp, P(vp), P(i64), P(vp), P(i64), P(vp))
 _sig("rq_save_mesh_dat", C.c_int, cp, vp, i64, vp, i64, vp)
 _sig("rq_load_samplecache_dat", C.c_int, cp, P(i32), P(i32), P(vp), P(vp), P(vp))
@@ -153,12 +144,24 @@ _sig("rq_save_samplecache_dat", C.c_int, cp, i32, i32, vp, vp, vp)
 _sig("rq_free_host", None, vp)
 _sig("rq_host_bvh_save", C.c_int, vp, cp)
 _sig("rq_host_bvh_load", C.c_int, cp, P(vp))
+_sig("rq_build_scene_gpu", C.c_int, vp, i64, vp, i64, C.c_int, P(vp), vp)
+_sig("rq_scene_sizes", C.c_int, vp, P(i64), P(i64), P(i64))
+# rays and AO
+_sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)
+_sig("rq_camera_rays", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, f32, f32, vp, vp)
+_sig("rq_surfels_from_hits", C.c_int, vp, vp, vp, i64, vp, vp, vp, vp)
+_sig("rq_probe_l2_read", C.c_int, vp, i64, C.c_int, vp, vp)
 _sig("rq_trace_ao", C.c_int, vp, vp, vp, i64, C.c_int, vp, P(Launch), vp)
+# instancing
 _sig("rq_tlas_create", C.c_int, P(vp), C.c_int, vp, vp, i64, P(vp))
 _sig("rq_tlas_destroy", C.c_int, vp)
 _sig("rq_tlas_buffers", C.c_int, vp, P(vp), P(i64), P(vp), P(i64), P(vp))
 _sig("rq_trace_instanced", C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, P(Launch), vp)
 _sig("rq_tlas_build_host", C.c_int, vp, C.c_int, vp, vp, i64, P(vp))
+# serving
 _sig("rq_server_submit_bake", C.c_int, vp, i32, vp, vp, vp, i64, C.c_int, u64, f32, f32, f32, vp, P(u64))
-_sig("rq_build_scene_gpu", C.c_int, vp, i64, vp, i64, C.c_int, P(vp), vp)
-_sig("rq_scene_sizes", C.c_int, vp, P(i64), P(i64), P(i64))
+
+
+def check(status: int, where: str) -> None:
+    if status != RQ_OK:
+        raise RQError(status, where)
