@@ -9,6 +9,12 @@
 
 #include "host_common.h"
 
+// SAH treelet passes over the binary tree of a CWBVH build when the caller
+// asks for the default.
+#ifndef RQ_DEFAULT_TREELET_PASSES
+#define RQ_DEFAULT_TREELET_PASSES 2
+#endif
+
 using namespace rq;
 
 
@@ -57,13 +63,14 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
     if (nt > (int64_t)INT32_MAX / 3) return RQ_ERR_INVALID_ARG;
     for (int64_t k = 0; k < 3 * nt; ++k)
         if (indices[k] < 0 || indices[k] >= nv) return RQ_ERR_INVALID_ARG;
-    rq_build_params bp{4, 32, 30, 0, 1};
+    rq_build_params bp{4, 32, 30, 0, 1, RQ_DEFAULT_TREELET_PASSES};
     if (params) {
         if (params->max_leaf_size > 0) bp.max_leaf_size = params->max_leaf_size;
         if (params->sah_bins > 0) bp.sah_bins = params->sah_bins;
         if (params->max_depth > 0) bp.max_depth = params->max_depth;
         bp.threads = params->threads;
         if (params->presplit > 0) bp.presplit = params->presplit;
+        if (params->treelet_passes != 0) bp.treelet_passes = std::max(0, params->treelet_passes);
     }
     if (bp.presplit != 1 && bp.presplit != 2 && bp.presplit != 4 && bp.presplit != 8) return RQ_ERR_INVALID_ARG;
     rq_host_bvh* h = new (std::nothrow) rq_host_bvh();
@@ -82,6 +89,8 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
             // The 8-wide tree's leaves hold at most 3 triangles (3 meta bits).
             const auto t0 = std::chrono::steady_clock::now();
             build_bvh2_tree(m, 3, bp.sah_bins, 48, false, bp.threads, h->b.tree2, bp.presplit);
+            const auto t1a = std::chrono::steady_clock::now();
+            treelet_optimize(h->b.tree2, bp.treelet_passes, bp.threads);
             const auto t1 = std::chrono::steady_clock::now();
             collapse_to_bvh8(h->b.tree2, h->b.tree8, bp.threads);
             const auto t2 = std::chrono::steady_clock::now();
@@ -90,8 +99,9 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
             h->b.depth = tree_depth8(h->b.tree8);
             if (std::getenv("RQ_LOG")) {
                 auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
-                std::fprintf(stderr, "rq_build_bvh: %lld tris, binary SAH %.1f ms, 8-wide collapse %.1f ms, "
-                             "CWBVH conversion %.1f ms\n", (long long)nt, ms(t0, t1), ms(t1, t2), ms(t2, t3));
+                std::fprintf(stderr, "rq_build_bvh: %lld tris, binary SAH %.1f ms, %d treelet passes %.1f ms, "
+                             "8-wide collapse %.1f ms, CWBVH conversion %.1f ms\n", (long long)nt, ms(t0, t1a),
+                             bp.treelet_passes, ms(t1a, t1), ms(t1, t2), ms(t2, t3));
             }
         }
     } catch (const std::bad_alloc&) {

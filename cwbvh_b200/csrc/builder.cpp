@@ -413,6 +413,189 @@ void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_dept
     build_from_refs(std::move(refs), 1, bins, max_depth, false, threads, out);
 }
 
+// ------------------------------------------------- treelet restructuring --
+// Karras and Aila, "Fast Parallel Construction of High-Quality Bounding
+// Volume Hierarchies" (HPG 2013), on the host's binary tree: at every inner
+// node, bottom-up, a treelet of up to 7 leaves is grown by repeatedly opening
+// its largest-area inner leaf; the binary topology over those leaves with the
+// least SAH cost is found by dynamic programming over the 127 leaf subsets,
+// and the treelet's inner nodes are rewired to it when that is cheaper.  The
+// top-down binned build judges each split only by the bounds it sees at that
+// level; rewiring fixes splits that later levels show to be poor (on terrain
+// with thin overlapping boxes, far fewer nodes are entered per ray).  Leaves
+// and their triangles are untouched, so every answer is the same.
+namespace {
+constexpr int kTreeletLeaves = 7;
+
+struct TreeletOpt {
+    Tree<2>& t;
+    std::vector<float> cost;  // SAH cost of each inner node's subtree
+
+    explicit TreeletOpt(Tree<2>& tree) : t(tree), cost(tree.nodes.size(), 0.f) {}
+
+    static float area(const BBox& b) { return b.area(); }
+    static BBox child_box(const TreeNode<2>& nd, int c) {
+        BBox b;
+        b.grow(nd.lo[c], nd.hi[c]);
+        return b;
+    }
+    float code_cost(int32_t code, float a) const {
+        return code >= 0 ? cost[(size_t)code] : kIntersectCost * a * (float)t.leaves[-code - 2].count;
+    }
+    void update_cost(int32_t v) {
+        const TreeNode<2>& nd = t.nodes[v];
+        const BBox b0 = child_box(nd, 0), b1 = child_box(nd, 1);
+        BBox b = b0;
+        b.grow(b1);
+        cost[(size_t)v] = kTraversalCost * b.area() + code_cost(nd.child[0], b0.area()) +
+                          code_cost(nd.child[1], b1.area());
+    }
+
+    // Rewires the treelet rooted at v; v keeps its index and its box.
+    void restructure(int32_t v) {
+        int32_t code[kTreeletLeaves];
+        BBox box[kTreeletLeaves];
+        int32_t inner[kTreeletLeaves - 1];
+        int nl = 2, ni = 1;
+        inner[0] = v;
+        for (int c = 0; c < 2; ++c) {
+            code[c] = t.nodes[v].child[c];
+            box[c] = child_box(t.nodes[v], c);
+        }
+        while (nl < kTreeletLeaves) {
+            int pick = -1;
+            float best_area = -1.f;
+            for (int i = 0; i < nl; ++i)
+                if (code[i] >= 0 && box[i].area() > best_area) { best_area = box[i].area(); pick = i; }
+            if (pick < 0) break;
+            const TreeNode<2>& nd = t.nodes[code[pick]];
+            inner[ni++] = code[pick];
+            code[nl] = nd.child[1];
+            box[nl] = child_box(nd, 1);
+            code[pick] = nd.child[0];
+            box[pick] = child_box(nd, 0);
+            ++nl;
+        }
+        if (nl < 3) return;  // two leaves have one topology
+        const unsigned full = (1u << nl) - 1u;
+        BBox sbox[1 << kTreeletLeaves];
+        float copt[1 << kTreeletLeaves];
+        uint8_t part[1 << kTreeletLeaves];
+        // A proper subset is numerically smaller than its set, so ascending
+        // order has every part's cost ready.
+        for (unsigned s = 1; s <= full; ++s) {
+            const unsigned low = s & (0u - s);
+            if (s == low) {
+                const int i = __builtin_ctz(s);
+                sbox[s] = box[i];
+                copt[s] = code_cost(code[i], box[i].area());
+                part[s] = 0;
+                continue;
+            }
+            sbox[s] = sbox[s ^ low];
+            sbox[s].grow(sbox[low]);
+            float best = INFINITY;
+            unsigned bp = 0;
+            // each unordered split once: the part that holds the lowest leaf
+            for (unsigned p = (s - 1u) & s; p; p = (p - 1u) & s) {
+                if (!(p & low)) continue;
+                const float c = copt[p] + copt[s ^ p];
+                if (c < best) { best = c; bp = p; }
+            }
+            copt[s] = kTraversalCost * sbox[s].area() + best;
+            part[s] = (uint8_t)bp;
+        }
+        // Keep the current treelet unless the new one is clearly cheaper
+        // (also when a cost is not finite).
+        if (!(copt[full] < cost[(size_t)v] * (1.f - 1e-6f))) return;
+        int used = 0;
+        emit(full, code, sbox, copt, part, inner, used);
+    }
+
+    int32_t emit(unsigned s, const int32_t* code, const BBox* sbox, const float* copt, const uint8_t* part,
+                 const int32_t* inner, int& used) {
+        if ((s & (s - 1u)) == 0u) return code[__builtin_ctz(s)];
+        const int32_t me = inner[used++];
+        const unsigned p = part[s];
+        const int32_t c0 = emit(p, code, sbox, copt, part, inner, used);
+        const int32_t c1 = emit(s ^ p, code, sbox, copt, part, inner, used);
+        TreeNode<2>& nd = t.nodes[me];
+        nd.child[0] = c0;
+        nd.child[1] = c1;
+        for (int a = 0; a < 3; ++a) {
+            nd.lo[0][a] = sbox[p].lo[a];
+            nd.hi[0][a] = sbox[p].hi[a];
+            nd.lo[1][a] = sbox[s ^ p].lo[a];
+            nd.hi[1][a] = sbox[s ^ p].hi[a];
+        }
+        cost[(size_t)me] = copt[s];
+        return me;
+    }
+
+    void post_order(int32_t root, std::vector<int32_t>& order) const {
+        std::vector<std::pair<int32_t, bool>> st{{root, false}};
+        while (!st.empty()) {
+            auto [v, done] = st.back();
+            st.pop_back();
+            if (done) {
+                order.push_back(v);
+                continue;
+            }
+            st.push_back({v, true});
+            for (int c = 0; c < 2; ++c)
+                if (t.nodes[v].child[c] >= 0) st.push_back({t.nodes[v].child[c], false});
+        }
+    }
+
+    // Costs bottom-up, then the treelet of every inner node with its subtree
+    // already done.  A restructure at v only rewires v's subtree, so subtrees
+    // below a depth cut run on worker threads and the nodes above them
+    // follow in reverse pre-order; the result is the same for any thread count.
+    void pass(int threads) {
+        const size_t n = t.nodes.size();
+        auto visit = [&](int32_t v) {
+            update_cost(v);
+            restructure(v);
+        };
+        if (threads == 1 || n < 65536) {
+            std::vector<int32_t> order;
+            order.reserve(n);
+            post_order(0, order);
+            for (int32_t v : order) visit(v);
+            return;
+        }
+        int depth_cut = 3;
+        while ((1 << depth_cut) < 8 * threads) ++depth_cut;
+        std::vector<int32_t> frontier, top;
+        std::vector<std::pair<int32_t, int>> st{{0, 0}};
+        while (!st.empty()) {
+            const auto [v, d] = st.back();
+            st.pop_back();
+            if (d == depth_cut) {
+                frontier.push_back(v);
+                continue;
+            }
+            top.push_back(v);
+            for (int c = 0; c < 2; ++c)
+                if (t.nodes[v].child[c] >= 0) st.push_back({t.nodes[v].child[c], d + 1});
+        }
+        parallel_tasks((int64_t)frontier.size(), threads, [&](int64_t i) {
+            std::vector<int32_t> sub;
+            post_order(frontier[(size_t)i], sub);
+            for (int32_t v : sub) visit(v);
+        });
+        for (auto it = top.rbegin(); it != top.rend(); ++it) visit(*it);
+    }
+};
+}  // namespace
+
+void treelet_optimize(Tree<2>& t, int passes, int threads) {
+    if (passes <= 0 || t.root_is_leaf || t.nodes.empty()) return;
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    TreeletOpt opt(t);
+    for (int p = 0; p < passes; ++p) opt.pass(threads);
+}
+
 // Optimal collapse of a binary tree into an 8-wide tree under a surface-area
 // cost model.  For every binary node n and k = 1..8, best[n][k] is the least
 // cost of representing the subtree of n with at most k children ("slots") of

@@ -134,6 +134,9 @@ void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool 
 // Binary tree over axis-aligned boxes (lo xyz, hi xyz per box; box k is
 // primitive k), e.g. the world bounds of instances for a top-level tree.
 void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_depth, int threads, Tree<2>& out);
+// SAH treelet restructuring of a binary tree (7-leaf treelets, `passes`
+// bottom-up sweeps); leaves and their primitives are unchanged.
+void treelet_optimize(Tree<2>& t, int passes, int threads);
 void collapse_to_bvh8(const Tree<2>& t2, Tree<8>& out, int threads = 1);
 int tree_depth2(const Tree<2>& t);
 int tree_depth8(const Tree<8>& t);

@@ -224,3 +224,39 @@ def test_build_independent_of_thread_count(rq, kind):
         assert np.array_equal(a.nodes.view(np.uint32), b.nodes.view(np.uint32))
         assert np.array_equal(a.woop.view(np.uint32), b.woop.view(np.uint32))
         assert np.array_equal(a.prim_index, b.prim_index)
+
+
+def test_treelets_keep_results_and_cut_visits(rq, po):
+    """SAH treelet restructuring of the binary tree only rewires inner nodes:
+    every AO ray gets the same occlusion bit and the same closest triangle
+    (up to ties explained in FP64), every triangle stays referenced once, and
+    on the heightfield-and-boxes family far fewer nodes are entered per ray."""
+    from cwbvh_b200 import workloads as W
+    from adjudicate import _explained, prim_ids
+    V, I = W.scene_of_size(3, 150_000)
+    rng = np.random.default_rng(6)
+    n = 20000
+    tri = rng.integers(0, I.shape[0], n)
+    a, b = np.sqrt(rng.random(n)), rng.random(n)
+    p0, p1, p2 = V[I[tri, 0]], V[I[tri, 1]], V[I[tri, 2]]
+    P = p0 * (1 - a)[:, None] + p1 * (a * (1 - b))[:, None] + p2 * (a * b)[:, None]
+    Nn = np.cross(p1 - p0, p2 - p0)
+    Nn /= np.maximum(np.linalg.norm(Nn, axis=1, keepdims=True), 1e-30)
+    pos = np.concatenate([P, np.ones((n, 1))], 1).astype(np.float32)
+    nrm = np.concatenate([Nn, np.zeros((n, 1))], 1).astype(np.float32)
+    d = W.diag(V)
+    rays = po.aorays(pos, nrm, np.zeros(n, np.float32), 1, 7, 1e-4 * d, 0.1 * d, 0.0)
+    plain = rq.HostBVH(V, I, rq.CWBVH, treelet_passes=-1)
+    opt = rq.HostBVH(V, I, rq.CWBVH)  # default passes
+    tr = opt.tree()
+    assert np.array_equal(np.sort(tr["prim_refs"]), np.arange(I.shape[0]))
+    assert tr["leaf_count"].max() <= 3
+    for any_hit in (True, False):
+        ha, va, _ = po.trace(0, plain.nodes, plain.woop, rays, any_hit, counts=True)
+        hb, vb, _ = po.trace(0, opt.nodes, opt.woop, rays, any_hit, counts=True)
+        x, y = prim_ids(ha, plain.prim_index), prim_ids(hb, opt.prim_index)
+        assert np.array_equal(x >= 0, y >= 0)
+        if not any_hit:
+            bad = np.nonzero(x != y)[0]
+            assert all(_explained(po, rays[k], V, I, (int(x[k]), int(y[k]))) for k in bad), len(bad)
+        assert vb.mean() < 0.85 * va.mean(), (vb.mean(), va.mean())
