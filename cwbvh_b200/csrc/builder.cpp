@@ -496,11 +496,14 @@ struct TreeletOpt {
             sbox[s].grow(sbox[low]);
             float best = INFINITY;
             unsigned bp = 0;
-            // each unordered split once: the part that holds the lowest leaf
-            for (unsigned p = (s - 1u) & s; p; p = (p - 1u) & s) {
-                if (!(p & low)) continue;
+            // each unordered split once: p holds the lowest leaf plus a proper
+            // subset q of the others
+            const unsigned rest = s ^ low;
+            for (unsigned q = (rest - 1u) & rest;; q = (q - 1u) & rest) {
+                const unsigned p = q | low;
                 const float c = copt[p] + copt[s ^ p];
                 if (c < best) { best = c; bp = p; }
+                if (q == 0u) break;
             }
             copt[s] = kTraversalCost * sbox[s].area() + best;
             part[s] = (uint8_t)bp;
