@@ -429,9 +429,10 @@ constexpr int kTreeletLeaves = 7;
 
 struct TreeletOpt {
     Tree<2>& t;
-    std::vector<float> cost;  // SAH cost of each inner node's subtree
+    std::vector<float> cost;      // SAH cost of each inner node's subtree
+    std::vector<uint8_t> dirty;   // the subtree changed in the latest pass that visited it
 
-    explicit TreeletOpt(Tree<2>& tree) : t(tree), cost(tree.nodes.size(), 0.f) {}
+    explicit TreeletOpt(Tree<2>& tree) : t(tree), cost(tree.nodes.size(), 0.f), dirty(tree.nodes.size(), 1) {}
 
     static float area(const BBox& b) { return b.area(); }
     static BBox child_box(const TreeNode<2>& nd, int c) {
@@ -451,8 +452,9 @@ struct TreeletOpt {
                           code_cost(nd.child[1], b1.area());
     }
 
-    // Rewires the treelet rooted at v; v keeps its index and its box.
-    void restructure(int32_t v) {
+    // Rewires the treelet rooted at v (v keeps its index and its box) and
+    // marks its inner nodes dirty; false when the treelet is kept.
+    bool restructure(int32_t v) {
         int32_t code[kTreeletLeaves];
         BBox box[kTreeletLeaves];
         int32_t inner[kTreeletLeaves - 1];
@@ -476,7 +478,7 @@ struct TreeletOpt {
             box[pick] = child_box(nd, 0);
             ++nl;
         }
-        if (nl < 3) return;  // two leaves have one topology
+        if (nl < 3) return false;  // two leaves have one topology
         const unsigned full = (1u << nl) - 1u;
         BBox sbox[1 << kTreeletLeaves];
         float copt[1 << kTreeletLeaves];
@@ -510,9 +512,11 @@ struct TreeletOpt {
         }
         // Keep the current treelet unless the new one is clearly cheaper
         // (also when a cost is not finite).
-        if (!(copt[full] < cost[(size_t)v] * (1.f - 1e-6f))) return;
+        if (!(copt[full] < cost[(size_t)v] * (1.f - 1e-6f))) return false;
         int used = 0;
         emit(full, code, sbox, copt, part, inner, used);
+        for (int k = 0; k < ni; ++k) dirty[(size_t)inner[k]] = 1;
+        return true;
     }
 
     int32_t emit(unsigned s, const int32_t* code, const BBox* sbox, const float* copt, const uint8_t* part,
@@ -535,7 +539,10 @@ struct TreeletOpt {
         return me;
     }
 
+    // Post-order of the dirty part of the subtree of `root` (a clean node's
+    // subtree is clean).
     void post_order(int32_t root, std::vector<int32_t>& order) const {
+        if (!dirty[(size_t)root]) return;
         std::vector<std::pair<int32_t, bool>> st{{root, false}};
         while (!st.empty()) {
             auto [v, done] = st.back();
@@ -545,20 +552,29 @@ struct TreeletOpt {
                 continue;
             }
             st.push_back({v, true});
-            for (int c = 0; c < 2; ++c)
-                if (t.nodes[v].child[c] >= 0) st.push_back({t.nodes[v].child[c], false});
+            for (int c = 0; c < 2; ++c) {
+                const int32_t ch = t.nodes[v].child[c];
+                if (ch >= 0 && dirty[(size_t)ch]) st.push_back({ch, false});
+            }
         }
     }
 
     // Costs bottom-up, then the treelet of every inner node with its subtree
-    // already done.  A restructure at v only rewires v's subtree, so subtrees
-    // below a depth cut run on worker threads and the nodes above them
-    // follow in reverse pre-order; the result is the same for any thread count.
+    // already done.  A node whose subtree did not change in the previous pass
+    // (and whose own treelet was kept) would keep it again, so only dirty
+    // nodes are visited.  A restructure at v only rewires v's subtree, so
+    // subtrees below a depth cut run on worker threads and the nodes above
+    // them follow in reverse pre-order; the result is the same for any
+    // thread count.
     void pass(int threads) {
         const size_t n = t.nodes.size();
         auto visit = [&](int32_t v) {
+            if (!dirty[(size_t)v]) return;
             update_cost(v);
-            restructure(v);
+            if (restructure(v)) return;  // marked dirty by the rewiring
+            const TreeNode<2>& nd = t.nodes[v];
+            dirty[(size_t)v] = (uint8_t)((nd.child[0] >= 0 && dirty[(size_t)nd.child[0]]) ||
+                                         (nd.child[1] >= 0 && dirty[(size_t)nd.child[1]]));
         };
         if (threads == 1 || n < 65536) {
             std::vector<int32_t> order;
