@@ -12,7 +12,7 @@
 // SAH treelet passes over the binary tree of a CWBVH build when the caller
 // asks for the default.
 #ifndef RQ_DEFAULT_TREELET_PASSES
-#define RQ_DEFAULT_TREELET_PASSES 2
+#define RQ_DEFAULT_TREELET_PASSES 4
 #endif
 
 using namespace rq;

@@ -88,7 +88,7 @@ typedef struct rq_build_params {
     int presplit;         /* 1, 2, 4 or 8: cut badly fitting triangles into up to this     */
                           /* many references with clipped boxes before the build (0 = 1)   */
     int treelet_passes;   /* CWBVH: passes of SAH treelet restructuring of the binary tree */
-                          /* before the 8-wide collapse (0 = default 2, negative = none)   */
+                          /* before the 8-wide collapse (0 = default 4, negative = none)   */
 } rq_build_params;
 
 typedef struct rq_bvh_info {
