@@ -176,7 +176,7 @@ class HostBVH:
 
     def __init__(self, vertices, indices, kind: int = CWBVH, max_leaf_size: int = 0, sah_bins: int = 0,
                  max_depth: int = 0, threads: int = 0, tree: Optional[dict] = None, presplit: int = 0,
-                 treelet_passes: int = 0):
+                 treelet_passes: int = 0, spatial_splits: int = 0):
         """Build with the library's SAH builder, or -- with `tree` (the dict
         shape of HostBVH.tree()) -- convert a tree built elsewhere."""
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
@@ -184,7 +184,7 @@ class HostBVH:
         self.vertices, self.indices, self.kind = v, i, kind
         h = C.c_void_p()
         if tree is None:
-            bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads, presplit, treelet_passes)
+            bp = N.BuildParams(max_leaf_size, sah_bins, max_depth, threads, presplit, treelet_passes, spatial_splits)
             check(lib.rq_build_bvh(v.ctypes.data, v.shape[0], i.ctypes.data, i.shape[0], kind, C.byref(bp),
                                    C.byref(h)), "rq_build_bvh")
         else:

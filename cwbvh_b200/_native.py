@@ -48,7 +48,7 @@ class Launch(C.Structure):
 
 class BuildParams(C.Structure):
     _fields_ = [("max_leaf_size", C.c_int), ("sah_bins", C.c_int), ("max_depth", C.c_int), ("threads", C.c_int),
-                ("presplit", C.c_int), ("treelet_passes", C.c_int)]
+                ("presplit", C.c_int), ("treelet_passes", C.c_int), ("spatial_splits", C.c_int)]
 
 
 class BVHInfo(C.Structure):

@@ -14,6 +14,11 @@
 #ifndef RQ_DEFAULT_TREELET_PASSES
 #define RQ_DEFAULT_TREELET_PASSES 4
 #endif
+// Spatial-split budget (duplicate references, percent of the triangles) when
+// the caller asks for the default.
+#ifndef RQ_DEFAULT_SPATIAL_SPLITS
+#define RQ_DEFAULT_SPATIAL_SPLITS 0
+#endif
 
 using namespace rq;
 
@@ -63,7 +68,7 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
     if (nt > (int64_t)INT32_MAX / 3) return RQ_ERR_INVALID_ARG;
     for (int64_t k = 0; k < 3 * nt; ++k)
         if (indices[k] < 0 || indices[k] >= nv) return RQ_ERR_INVALID_ARG;
-    rq_build_params bp{4, 32, 30, 0, 1, RQ_DEFAULT_TREELET_PASSES};
+    rq_build_params bp{4, 32, 30, 0, 1, RQ_DEFAULT_TREELET_PASSES, RQ_DEFAULT_SPATIAL_SPLITS};
     if (params) {
         if (params->max_leaf_size > 0) bp.max_leaf_size = params->max_leaf_size;
         if (params->sah_bins > 0) bp.sah_bins = params->sah_bins;
@@ -71,8 +76,11 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
         bp.threads = params->threads;
         if (params->presplit > 0) bp.presplit = params->presplit;
         if (params->treelet_passes != 0) bp.treelet_passes = std::max(0, params->treelet_passes);
+        if (params->spatial_splits != 0) bp.spatial_splits = std::max(0, params->spatial_splits);
     }
     if (bp.presplit != 1 && bp.presplit != 2 && bp.presplit != 4 && bp.presplit != 8) return RQ_ERR_INVALID_ARG;
+    if (bp.spatial_splits > 400) return RQ_ERR_INVALID_ARG;
+    const float split_budget = 0.01f * (float)bp.spatial_splits;
     rq_host_bvh* h = new (std::nothrow) rq_host_bvh();
     if (!h) return RQ_ERR_OOM;
     try {
@@ -82,13 +90,13 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
         h->b.kind = kind;
         if (kind == RQ_BVH_BVH2) {
             build_bvh2_tree(m, std::max(1, bp.max_leaf_size), bp.sah_bins, bp.max_depth, true, bp.threads, h->b.tree2,
-                            bp.presplit);
+                            bp.presplit, split_budget);
             convert_bvh2(h->b.tree2, m, h->b);
             h->b.depth = tree_depth2(h->b.tree2);
         } else {
             // The 8-wide tree's leaves hold at most 3 triangles (3 meta bits).
             const auto t0 = std::chrono::steady_clock::now();
-            build_bvh2_tree(m, 3, bp.sah_bins, 48, false, bp.threads, h->b.tree2, bp.presplit);
+            build_bvh2_tree(m, 3, bp.sah_bins, 48, false, bp.threads, h->b.tree2, bp.presplit, split_budget);
             const auto t1a = std::chrono::steady_clock::now();
             treelet_optimize(h->b.tree2, bp.treelet_passes, bp.threads);
             const auto t1 = std::chrono::steady_clock::now();

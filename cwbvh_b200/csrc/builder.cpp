@@ -61,15 +61,75 @@ inline void centroid(const PrimRef& p, float c[3]) {
     for (int a = 0; a < 3; ++a) c[a] = (p.lo[a] + p.hi[a]) * 0.5f;
 }
 
+// Box of the part of triangle `tri` (vertices v[0..2]) that lies in the slab
+// lo <= x[axis] <= hi, intersected with `clip`.  Edge/plane intersections are
+// computed in double and rounded outwards, so the box contains the exact
+// part; false when the part is empty.
+bool slab_box(const float (*v)[3], int axis, float lo, float hi, const BBox& clip, BBox& out) {
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    bool any = false;
+    auto grow = [&](const double* q) {
+        for (int a = 0; a < 3; ++a) { mn[a] = std::min(mn[a], q[a]); mx[a] = std::max(mx[a], q[a]); }
+        any = true;
+    };
+    for (int e = 0; e < 3; ++e) {
+        const float* p = v[e];
+        const float* q = v[(e + 1) % 3];
+        if (p[axis] >= lo && p[axis] <= hi) {
+            const double d[3] = {p[0], p[1], p[2]};
+            grow(d);
+        }
+        for (const float plane : {lo, hi}) {
+            if (!std::isfinite(plane)) continue;
+            const double dp = (double)p[axis] - plane, dq = (double)q[axis] - plane;
+            if (!((dp < 0.0 && dq > 0.0) || (dp > 0.0 && dq < 0.0))) continue;
+            const double t = dp / (dp - dq);
+            double x[3];
+            for (int a = 0; a < 3; ++a) x[a] = (double)p[a] + t * ((double)q[a] - (double)p[a]);
+            x[axis] = plane;
+            grow(x);
+        }
+    }
+    if (!any) return false;
+    for (int a = 0; a < 3; ++a) {
+        float l = (float)mn[a], h = (float)mx[a];
+        if ((double)l > mn[a]) l = std::nextafter(l, -INFINITY);
+        if ((double)h < mx[a]) h = std::nextafter(h, INFINITY);
+        if (a == axis) { l = fmx(l, lo); h = fmn(h, hi); }
+        out.lo[a] = fmx(l, clip.lo[a]);
+        out.hi[a] = fmn(h, clip.hi[a]);
+        if (out.lo[a] > out.hi[a]) return false;
+    }
+    return true;
+}
+
 struct Builder2 {
     int max_leaf, bins, max_depth;
     bool big_leaves;  // at the depth cap: one oversized leaf (BVH2) or median splits (CWBVH source)
+    // Spatial splits (Stich, Friedrich and Dietrich, "Spatial Splits in
+    // Bounding Volume Hierarchies", HPG 2009) need the triangles; they are
+    // tried where the object split's children overlap by more than
+    // split_alpha of the root's area.
+    const Mesh* mesh = nullptr;
+    float split_alpha = 1e-5f;
+    float root_area = 0.f;
+    int spatial_bins = 8;
+    int64_t spatial_min = 0;  // nodes with fewer references use object splits only
+    // refs[begin, end) are a node's references and refs[end, cap) the slack
+    // its subtree may fill with spatial-split duplicates; slack is handed to
+    // the children in proportion to their sizes, so the tree does not depend
+    // on the order in which subtrees are built.
     std::vector<PrimRef> refs;
     std::vector<TreeNode<2>> nodes;
     std::vector<Leaf> leaves;
     std::atomic<int32_t> n_nodes{0};
     std::atomic<int32_t> n_leaves{0};
     std::atomic<int> spare_threads{0};
+
+    struct Range {
+        int64_t begin, end, cap;
+        BBox box, cbox;
+    };
 
     int32_t make_leaf(int64_t begin, int64_t end) {
         // Fragments of one split triangle can share a leaf: keep one of each.
@@ -84,13 +144,36 @@ struct Builder2 {
         return -(l + 2);
     }
 
-    // Child code of the subtree over refs[begin, end) with bounds `b` and
-    // centroid bounds `cb`.
-    int32_t build(int64_t begin, int64_t end, const BBox& b, const BBox& cb, int depth) {
+    void tri_verts(int32_t id, float v[3][3]) const {
+        for (int k = 0; k < 3; ++k)
+            for (int a = 0; a < 3; ++a) v[k][a] = mesh->v[3 * (size_t)mesh->i[3 * (int64_t)id + k] + a];
+    }
+
+    // Bounds of refs[begin, end) and of their centroids.
+    void bounds_of(int64_t begin, int64_t end, BBox& b, BBox& cb) const {
+        b = BBox();
+        cb = BBox();
+        for (int64_t k = begin; k < end; ++k) {
+            float c[3];
+            centroid(refs[k], c);
+            b.grow(refs[k].lo, refs[k].hi);
+            cb.grow_pt(c);
+        }
+    }
+
+    // Splits the slack of [begin, cap) between children of nl and nr
+    // references placed at begin: returns the left child's slack.
+    static int64_t left_slack(int64_t slack, int64_t nl, int64_t nr) {
+        return slack <= 0 ? 0 : (int64_t)((__int128)slack * nl / (nl + nr));
+    }
+
+    // Child code of the subtree over refs[begin, end) with slack up to cap,
+    // bounds `b` and centroid bounds `cb`.
+    int32_t build(int64_t begin, int64_t end, int64_t cap, const BBox& b, const BBox& cb, int depth) {
         const int64_t n = end - begin;
         const bool may_leaf = n <= max_leaf;
         if (n == 1 || (depth >= max_depth && (may_leaf || big_leaves))) return make_leaf(begin, end);
-        if (depth >= max_depth) return median_split(begin, end, cb, depth);
+        if (depth >= max_depth) return median_split(begin, end, cap, cb, depth);
 
         // One pass: bin all three axes (fewer bins for small nodes: the bin
         // arrays are initialised per node).
@@ -147,7 +230,19 @@ struct Builder2 {
         const float split_cost =
             kTraversalCost + kIntersectCost * (parent_area > 0.f ? best_cost / parent_area : 0.f);
         if (may_leaf && (best_axis < 0 || kIntersectCost * (float)n <= split_cost)) return make_leaf(begin, end);
-        if (best_axis < 0) return median_split(begin, end, cb, depth);  // all centroids coincide
+
+        BBox lb, lcb, rb, rcb;
+        if (best_axis >= 0) {
+            for (int i = 0; i < nb; ++i) {
+                if (i <= best_bin) { lb.grow(bin[best_axis][i].box); lcb.grow(bin[best_axis][i].cbox); }
+                else { rb.grow(bin[best_axis][i].box); rcb.grow(bin[best_axis][i].cbox); }
+            }
+        }
+        int32_t code;
+        if (mesh && cap > end && try_spatial(begin, end, cap, b, best_axis >= 0 ? best_cost : INFINITY, lb, rb,
+                                             depth, best_axis >= 0, code))
+            return code;
+        if (best_axis < 0) return median_split(begin, end, cap, cb, depth);  // all centroids coincide
 
         const int a = best_axis;
         const float lo = cb.lo[a], sc = scale[a];
@@ -158,18 +253,173 @@ struct Builder2 {
             return bi <= best_bin;
         });
         const int64_t mid = begin + (m - first);
-        if (mid == begin || mid == end) return median_split(begin, end, cb, depth);
-        BBox lb, lcb, rb, rcb;
-        for (int i = 0; i < nb; ++i) {
-            if (i <= best_bin) { lb.grow(bin[a][i].box); lcb.grow(bin[a][i].cbox); }
-            else { rb.grow(bin[a][i].box); rcb.grow(bin[a][i].cbox); }
+        if (mid == begin || mid == end) return median_split(begin, end, cap, cb, depth);
+        return object_children(begin, mid, end, cap, lb, lcb, rb, rcb, depth);
+    }
+
+    // Children [begin, mid) and [mid, end) of an in-place partition; the
+    // right block moves up by the left child's slack.
+    int32_t object_children(int64_t begin, int64_t mid, int64_t end, int64_t cap, const BBox& lb, const BBox& lcb,
+                            const BBox& rb, const BBox& rcb, int depth) {
+        const int64_t sl = left_slack(cap - end, mid - begin, end - mid);
+        if (sl > 0) std::move_backward(refs.data() + mid, refs.data() + end, refs.data() + end + sl);
+        return make_inner(Range{begin, mid, mid + sl, lb, lcb}, Range{mid + sl, end + sl, cap, rb, rcb}, depth);
+    }
+
+    // Binned spatial split of refs[begin, end) (bins over the node's box);
+    // taken, with reference unsplitting, when cheaper than the object split
+    // and within the slack.  On success the node is built and its code
+    // returned in `code`.
+    bool try_spatial(int64_t begin, int64_t end, int64_t cap, const BBox& b, float object_cost, const BBox& olb,
+                     const BBox& orb, int depth, bool have_object, int32_t& code) {
+        const int64_t n = end - begin;
+        if (n < spatial_min) return false;
+        if (have_object) {
+            BBox ov;
+            for (int a = 0; a < 3; ++a) { ov.lo[a] = fmx(olb.lo[a], orb.lo[a]); ov.hi[a] = fmn(olb.hi[a], orb.hi[a]); }
+            if (!(ov.area() > split_alpha * root_area)) return false;
         }
-        return make_inner(begin, mid, end, lb, lcb, rb, rcb, depth);
+        const int nb = (int)std::min<int64_t>(spatial_bins, std::max<int64_t>(4, n));
+        struct SBin {
+            BBox box;
+            int enter = 0, exit = 0;
+        };
+        float best = object_cost;
+        int best_axis = -1, best_plane = -1;
+        int64_t best_nl = 0, best_nr = 0;
+        // Plane k of axis a (k = 0..nb); bin j lies between planes j and j+1.
+        float planes[3][kMaxBins + 1], to_bin[3];
+        for (int a = 0; a < 3; ++a) {
+            const float ext = b.hi[a] - b.lo[a];
+            for (int k = 0; k <= nb; ++k)
+                planes[a][k] = k == 0 ? b.lo[a] : (k == nb ? b.hi[a] : b.lo[a] + ext * ((float)k / (float)nb));
+            to_bin[a] = ext > 0.f ? (float)nb / ext : 0.f;
+        }
+        auto plane = [&](int a, int k) { return planes[a][k]; };
+        auto bin_of = [&](int a, float x) {
+            int k = (int)((x - b.lo[a]) * to_bin[a]);
+            k = k < 0 ? 0 : (k >= nb ? nb - 1 : k);
+            while (k > 0 && x < planes[a][k]) --k;
+            while (k < nb - 1 && x >= planes[a][k + 1]) ++k;
+            return k;
+        };
+        SBin sbin[3][kMaxBins];
+        bool usable[3];
+        for (int a = 0; a < 3; ++a) usable[a] = b.hi[a] - b.lo[a] > 0.f;
+        for (int64_t k = begin; k < end; ++k) {
+            const PrimRef& r = refs[k];
+            BBox rbox;
+            rbox.grow(r.lo, r.hi);
+            for (int a = 0; a < 3; ++a) {
+                if (!usable[a]) continue;
+                const int b0 = bin_of(a, r.lo[a]), b1 = bin_of(a, r.hi[a]);
+                sbin[a][b0].enter++;
+                sbin[a][b1].exit++;
+                for (int j = b0; j <= b1; ++j) {
+                    BBox q = rbox;
+                    q.lo[a] = fmx(q.lo[a], plane(a, j));
+                    q.hi[a] = fmn(q.hi[a], plane(a, j + 1));
+                    sbin[a][j].box.grow(q);
+                }
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (!usable[a]) continue;
+            const SBin* sb = sbin[a];
+            float right_area[kMaxBins];
+            int64_t right_count[kMaxBins];
+            BBox rb;
+            int64_t rc = 0;
+            for (int i = nb - 1; i > 0; --i) {
+                rb.grow(sb[i].box);
+                rc += sb[i].exit;
+                right_area[i] = rb.area();
+                right_count[i] = rc;
+            }
+            BBox lb;
+            int64_t lc = 0;
+            for (int i = 0; i < nb - 1; ++i) {
+                lb.grow(sb[i].box);
+                lc += sb[i].enter;
+                const int64_t nr = right_count[i + 1];
+                if (lc == 0 || nr == 0 || lc == n || nr == n) continue;
+                if (begin + lc + nr > cap) continue;  // over this subtree's budget
+                const float c = lb.area() * (float)lc + right_area[i + 1] * (float)nr;
+                if (c < best) { best = c; best_axis = a; best_plane = i + 1; best_nl = lc; best_nr = nr; }
+            }
+        }
+        if (best_axis < 0) return false;
+
+        // Distribute: wholly left / right, or straddling (split or unsplit).
+        const int a = best_axis;
+        const float pos = b.lo[a] + (b.hi[a] - b.lo[a]) * ((float)best_plane / (float)nb);
+        std::vector<PrimRef> left, right, straddle;
+        left.reserve((size_t)best_nl);
+        right.reserve((size_t)best_nr);
+        BBox lbox, rbox;
+        for (int64_t k = begin; k < end; ++k) {
+            const PrimRef& r = refs[k];
+            if (r.hi[a] <= pos) { left.push_back(r); lbox.grow(r.lo, r.hi); }
+            else if (r.lo[a] >= pos) { right.push_back(r); rbox.grow(r.lo, r.hi); }
+            else straddle.push_back(r);
+        }
+        for (size_t si = 0; si < straddle.size(); ++si) {
+            const PrimRef& r = straddle[si];
+            const int64_t still = (int64_t)(straddle.size() - si - 1);  // each takes >= 1 slot
+            BBox whole;
+            whole.grow(r.lo, r.hi);
+            float v[3][3];
+            tri_verts(r.id, v);
+            BBox lp, rp;
+            const bool hl = slab_box(v, a, -INFINITY, pos, whole, lp);
+            const bool hr = slab_box(v, a, pos, INFINITY, whole, rp);
+            const float nl = (float)left.size(), nr = (float)right.size();
+            BBox l_all = lbox, r_all = rbox;
+            l_all.grow(whole);
+            r_all.grow(whole);
+            BBox l_split = lbox, r_split = rbox;
+            if (hl) l_split.grow(lp);
+            if (hr) r_split.grow(rp);
+            const float c_split = hl && hr ? l_split.area() * (nl + 1) + r_split.area() * (nr + 1) : INFINITY;
+            const float c_left = l_all.area() * (nl + 1) + rbox.area() * nr;
+            const float c_right = lbox.area() * nl + r_all.area() * (nr + 1);
+            if (c_split < c_left && c_split < c_right &&
+                begin + (int64_t)left.size() + (int64_t)right.size() + 2 + still <= cap) {
+                PrimRef pl = r, pr = r;
+                for (int q = 0; q < 3; ++q) {
+                    pl.lo[q] = lp.lo[q]; pl.hi[q] = lp.hi[q];
+                    pr.lo[q] = rp.lo[q]; pr.hi[q] = rp.hi[q];
+                }
+                left.push_back(pl);
+                right.push_back(pr);
+                lbox.grow(lp);
+                rbox.grow(rp);
+            } else if (c_left <= c_right) {
+                left.push_back(r);
+                lbox.grow(whole);
+            } else {
+                right.push_back(r);
+                rbox.grow(whole);
+            }
+        }
+        const int64_t nl = (int64_t)left.size(), nr = (int64_t)right.size();
+        // Unsplitting emptied a side or kept every reference on one side:
+        // the node is left to the object split.
+        if (nl == 0 || nr == 0 || nl == n || nr == n || begin + nl + nr > cap) return false;
+        const int64_t sl = left_slack(cap - begin - nl - nr, nl, nr);
+        std::copy(left.begin(), left.end(), refs.data() + begin);
+        std::copy(right.begin(), right.end(), refs.data() + begin + nl + sl);
+        BBox lb, lcb, rb, rcb;
+        bounds_of(begin, begin + nl, lb, lcb);
+        bounds_of(begin + nl + sl, begin + nl + sl + nr, rb, rcb);
+        code = make_inner(Range{begin, begin + nl, begin + nl + sl, lb, lcb},
+                                    Range{begin + nl + sl, begin + nl + sl + nr, cap, rb, rcb}, depth);
+        return true;
     }
 
     // Balanced split at the centroid median of the widest centroid axis; keeps
     // the depth bounded by log2(n) once the SAH recursion reaches the cap.
-    int32_t median_split(int64_t begin, int64_t end, const BBox& cb, int depth) {
+    int32_t median_split(int64_t begin, int64_t end, int64_t cap, const BBox& cb, int depth) {
         int axis = 0;
         float widest = -1.f;
         for (int a = 0; a < 3; ++a)
@@ -180,18 +430,13 @@ struct Builder2 {
                              return x.lo[axis] + x.hi[axis] < y.lo[axis] + y.hi[axis];
                          });
         BBox lb, lcb, rb, rcb;
-        for (int64_t k = begin; k < end; ++k) {
-            float c[3];
-            centroid(refs[k], c);
-            if (k < mid) { lb.grow(refs[k].lo, refs[k].hi); lcb.grow_pt(c); }
-            else { rb.grow(refs[k].lo, refs[k].hi); rcb.grow_pt(c); }
-        }
-        return make_inner(begin, mid, end, lb, lcb, rb, rcb, depth);
+        bounds_of(begin, mid, lb, lcb);
+        bounds_of(mid, end, rb, rcb);
+        return object_children(begin, mid, end, cap, lb, lcb, rb, rcb, depth);
     }
 
-    int32_t make_inner(int64_t begin, int64_t mid, int64_t end, const BBox& lb, const BBox& lcb, const BBox& rb,
-                       const BBox& rcb, int depth) {
-        const int64_t n = end - begin;
+    int32_t make_inner(const Range& l, const Range& r, int depth) {
+        const int64_t n = (l.end - l.begin) + (r.end - r.begin);
         const int32_t me = n_nodes.fetch_add(1);
         int32_t lc, rc;
         bool spawned = false;
@@ -199,26 +444,27 @@ struct Builder2 {
         if (n > kParallelGrain) {
             if (spare_threads.fetch_sub(1) > 0) {
                 spawned = true;
-                fut = std::async(std::launch::async, [=, this] { return build(begin, mid, lb, lcb, depth + 1); });
+                fut = std::async(std::launch::async,
+                                 [=, this] { return build(l.begin, l.end, l.cap, l.box, l.cbox, depth + 1); });
             } else {
                 spare_threads.fetch_add(1);
             }
         }
         if (spawned) {
-            rc = build(mid, end, rb, rcb, depth + 1);
+            rc = build(r.begin, r.end, r.cap, r.box, r.cbox, depth + 1);
             lc = fut.get();
             spare_threads.fetch_add(1);
         } else {
-            lc = build(begin, mid, lb, lcb, depth + 1);
-            rc = build(mid, end, rb, rcb, depth + 1);
+            lc = build(l.begin, l.end, l.cap, l.box, l.cbox, depth + 1);
+            rc = build(r.begin, r.end, r.cap, r.box, r.cbox, depth + 1);
         }
         TreeNode<2> node{};
         node.count = 2;
         node.child[0] = lc;
         node.child[1] = rc;
         for (int a = 0; a < 3; ++a) {
-            node.lo[0][a] = lb.lo[a]; node.hi[0][a] = lb.hi[a];
-            node.lo[1][a] = rb.lo[a]; node.hi[1][a] = rb.hi[a];
+            node.lo[0][a] = l.box.lo[a]; node.hi[0][a] = l.box.hi[a];
+            node.lo[1][a] = r.box.lo[a]; node.hi[1][a] = r.box.hi[a];
         }
         nodes[me] = node;
         return me;
@@ -350,9 +596,10 @@ std::vector<PrimRef> make_refs(const Mesh& m, int max_frags) {
 
 }  // namespace
 
-static void build_from_refs(std::vector<PrimRef> refs, int max_leaf, int bins, int max_depth, bool big_leaves,
-                            int threads, Tree<2>& out) {
+static void build_from_refs(std::vector<PrimRef> refs, const Mesh* mesh, float split_budget, int max_leaf, int bins,
+                            int max_depth, bool big_leaves, int threads, Tree<2>& out) {
     Builder2 b;
+    b.mesh = split_budget > 0.f ? mesh : nullptr;
     b.max_leaf = max_leaf;
     b.big_leaves = big_leaves;
     b.bins = std::max(2, std::min(bins, kMaxBins));
@@ -368,8 +615,12 @@ static void build_from_refs(std::vector<PrimRef> refs, int max_leaf, int bins, i
         all.grow(p.lo, p.hi);
         call.grow_pt(c);
     }
-    b.nodes.resize(std::max<int64_t>(1, 2 * nt));
-    b.leaves.resize(std::max<int64_t>(1, nt));
+    // Spatial splits may add up to split_budget * nt duplicate references.
+    const int64_t cap = b.mesh ? nt + (int64_t)((double)split_budget * (double)nt) : nt;
+    b.refs.resize((size_t)cap);
+    b.root_area = all.area();
+    b.nodes.resize(std::max<int64_t>(1, cap));
+    b.leaves.resize(std::max<int64_t>(1, cap));
 
     out = Tree<2>();
     out.bounds.lo = v3(all.lo[0], all.lo[1], all.lo[2]);
@@ -379,24 +630,29 @@ static void build_from_refs(std::vector<PrimRef> refs, int max_leaf, int bins, i
         out.leaves.push_back(Leaf{0, 0});
         return;
     }
-    const int32_t root = b.build(0, nt, all, call, 0);
-    out.prim_refs.resize(nt);
-    for (int64_t t = 0; t < nt; ++t) out.prim_refs[t] = b.refs[t].id;
+    const int32_t root = b.build(0, nt, cap, all, call, 0);
+    // Slots are handed out in parallel; the root took slot 0.
+    b.nodes.resize(b.n_nodes.load());
+    b.leaves.resize(b.n_leaves.load());
+    // Leaves index refs with slack between subtrees: pack their references.
+    out.prim_refs.reserve((size_t)nt);
+    for (Leaf& l : b.leaves) {
+        const int32_t first = (int32_t)out.prim_refs.size();
+        for (int32_t k = 0; k < l.count; ++k) out.prim_refs.push_back(b.refs[(size_t)l.first + k].id);
+        l.first = first;
+    }
     if (root < 0) {
         out.root_is_leaf = true;
         out.leaves.push_back(b.leaves[-root - 2]);
         return;
     }
-    // Slots are handed out in parallel; the root took slot 0.
-    b.nodes.resize(b.n_nodes.load());
-    b.leaves.resize(b.n_leaves.load());
     out.nodes = std::move(b.nodes);
     out.leaves = std::move(b.leaves);
 }
 
 void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
-                     Tree<2>& out, int max_frags) {
-    build_from_refs(make_refs(m, max_frags), max_leaf, bins, max_depth, big_leaves, threads, out);
+                     Tree<2>& out, int max_frags, float split_budget) {
+    build_from_refs(make_refs(m, max_frags), &m, split_budget, max_leaf, bins, max_depth, big_leaves, threads, out);
 }
 
 void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_depth, int threads, Tree<2>& out) {
@@ -410,7 +666,7 @@ void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_dept
         p.id = (int32_t)k;
         p.pad = 0;
     }
-    build_from_refs(std::move(refs), 1, bins, max_depth, false, threads, out);
+    build_from_refs(std::move(refs), nullptr, 0.f, 1, bins, max_depth, false, threads, out);
 }
 
 // ------------------------------------------------- treelet restructuring --

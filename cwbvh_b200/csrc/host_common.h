@@ -128,9 +128,11 @@ struct HostBVH {
 
 // Builders (builder.cpp)
 // max_frags > 1: pre-split badly fitting triangles into up to max_frags
-// references with clipped bounds (power of two).
+// references with clipped bounds (power of two).  split_budget > 0: spatial
+// splits during the build, adding at most split_budget * triangles
+// duplicate references.
 void build_bvh2_tree(const Mesh& m, int max_leaf, int bins, int max_depth, bool big_leaves, int threads,
-                     Tree<2>& out, int max_frags = 1);
+                     Tree<2>& out, int max_frags = 1, float split_budget = 0.f);
 // Binary tree over axis-aligned boxes (lo xyz, hi xyz per box; box k is
 // primitive k), e.g. the world bounds of instances for a top-level tree.
 void build_bvh2_tree_boxes(const float* boxes, int64_t n, int bins, int max_depth, int threads, Tree<2>& out);

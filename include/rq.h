@@ -89,6 +89,9 @@ typedef struct rq_build_params {
                           /* many references with clipped boxes before the build (0 = 1)   */
     int treelet_passes;   /* CWBVH: passes of SAH treelet restructuring of the binary tree */
                           /* before the 8-wide collapse (0 = default 4, negative = none)   */
+    int spatial_splits;   /* binned spatial splits in the SAH build (as Embree's high-     */
+                          /* quality builder): budget of duplicate triangle references in  */
+                          /* percent of the triangle count (0 = default, negative = none)  */
 } rq_build_params;
 
 typedef struct rq_bvh_info {

@@ -260,3 +260,71 @@ def test_treelets_keep_results_and_cut_visits(rq, po):
             bad = np.nonzero(x != y)[0]
             assert all(_explained(po, rays[k], V, I, (int(x[k]), int(y[k]))) for k in bad), len(bad)
         assert vb.mean() < 0.85 * va.mean(), (vb.mean(), va.mean())
+
+
+def _ao_rays_numpy(po, V, I, n, seed):
+    from cwbvh_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    tri = rng.integers(0, I.shape[0], n)
+    a, b = np.sqrt(rng.random(n)), rng.random(n)
+    p0, p1, p2 = V[I[tri, 0]], V[I[tri, 1]], V[I[tri, 2]]
+    P = p0 * (1 - a)[:, None] + p1 * (a * (1 - b))[:, None] + p2 * (a * b)[:, None]
+    Nn = np.cross(p1 - p0, p2 - p0)
+    Nn /= np.maximum(np.linalg.norm(Nn, axis=1, keepdims=True), 1e-30)
+    pos = np.concatenate([P, np.ones((n, 1))], 1).astype(np.float32)
+    nrm = np.concatenate([Nn, np.zeros((n, 1))], 1).astype(np.float32)
+    d = W.diag(V)
+    return po.aorays(pos, nrm, np.zeros(n, np.float32), 1, seed, 1e-4 * d, 0.1 * d, 0.0)
+
+
+@pytest.mark.parametrize("kind", [0, 1], ids=["cwbvh", "bvh2"])
+def test_spatial_splits_keep_results(rq, po, kind):
+    """Spatial splits duplicate references to triangles that straddle a split
+    plane, with boxes clipped to each side: every AO ray gets the same
+    occlusion bit and the same closest triangle (ties explained in FP64),
+    every triangle is still referenced, each duplicate's Woop rows are its
+    triangle's, and on the heightfield-and-boxes family fewer nodes are
+    entered per ray."""
+    from cwbvh_b200 import workloads as W
+    from adjudicate import _explained, prim_ids
+    V, I = W.scene_of_size(3, 150_000)
+    rays = _ao_rays_numpy(po, V, I, 20000, 8)
+    plain = rq.HostBVH(V, I, kind, spatial_splits=-1)
+    split = rq.HostBVH(V, I, kind, spatial_splits=30)
+    if kind == rq.CWBVH:
+        tr = split.tree()
+        assert tr["leaf_count"].max() <= 3
+        n_refs = tr["prim_refs"].size
+        assert I.shape[0] < n_refs <= int(1.3 * I.shape[0]) + 1
+        assert np.array_equal(np.unique(tr["prim_refs"]), np.arange(I.shape[0]))
+        ids = split.prim_index.reshape(-1, 3)[:, 0]
+        rows = split.woop.reshape(-1, 3, 4)
+        for slot in np.random.default_rng(1).integers(0, ids.size, 200):
+            t = I[ids[slot]]
+            want = rq.woopify(V[t[0]], V[t[1]], V[t[2]])
+            assert np.array_equal(rows[slot].view(np.uint32), want.view(np.uint32))
+    for any_hit in (True, False):
+        ha, va, _ = po.trace(kind, plain.nodes, plain.woop, rays, any_hit, counts=True)
+        hb, vb, _ = po.trace(kind, split.nodes, split.woop, rays, any_hit, counts=True)
+        x, y = prim_ids(ha, plain.prim_index), prim_ids(hb, split.prim_index)
+        assert np.array_equal(x >= 0, y >= 0)
+        if not any_hit:
+            bad = np.nonzero(x != y)[0]
+            assert all(_explained(po, rays[k], V, I, (int(x[k]), int(y[k]))) for k in bad), len(bad)
+        if kind == rq.CWBVH:
+            assert vb.mean() < 0.95 * va.mean(), (vb.mean(), va.mean())
+
+
+def test_spatial_splits_independent_of_thread_count(rq):
+    """Slack for duplicates is handed to subtrees in proportion to their
+    sizes, so the spatial-split build is the same for any thread count."""
+    from cwbvh_b200 import workloads as W
+    V, I = W.scene_of_size(9, 200_000)
+    a = rq.HostBVH(V, I, rq.CWBVH, threads=1, spatial_splits=30)
+    for th in (3, 8):
+        b = rq.HostBVH(V, I, rq.CWBVH, threads=th, spatial_splits=30)
+        assert np.array_equal(a.nodes.view(np.uint32), b.nodes.view(np.uint32))
+        assert np.array_equal(a.woop.view(np.uint32), b.woop.view(np.uint32))
+        assert np.array_equal(a.prim_index, b.prim_index)
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        rq.HostBVH(V, I, rq.CWBVH, spatial_splits=1000)
