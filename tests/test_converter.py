@@ -198,14 +198,20 @@ def test_presplit_keeps_results(rq, po, presplit):
 
 
 def test_builder_invariants(rq):
-    """Leaves hold <= 3 triangles (CWBVH), every triangle is referenced once,
-    and the depth stays within the traversal stacks."""
+    """Leaves hold <= 3 triangles (CWBVH), every triangle is referenced (once
+    without spatial splits, at most once per leaf with them), and the depth
+    stays within the traversal stacks."""
     from cwbvh_b200 import workloads as W
     V, I = W.scene_of_size(4, 50_000)
     hb = rq.HostBVH(V, I, rq.CWBVH)
     tr = hb.tree()
     assert tr["leaf_count"].max() <= 3 and tr["leaf_count"].min() >= 1
-    assert np.array_equal(np.sort(tr["prim_refs"]), np.arange(I.shape[0]))
+    assert np.array_equal(np.unique(tr["prim_refs"]), np.arange(I.shape[0]))
+    assert tr["prim_refs"].size <= 2 * I.shape[0]
+    for f, c in zip(tr["leaf_first"], tr["leaf_count"]):
+        assert len(set(tr["prim_refs"][f:f + c].tolist())) == c
+    once = rq.HostBVH(V, I, rq.CWBVH, spatial_splits=-1).tree()
+    assert np.array_equal(np.sort(once["prim_refs"]), np.arange(I.shape[0]))
     assert 2 * hb.info["depth"] <= 64
     hb2 = rq.HostBVH(V, I, rq.BVH2)
     assert hb2.info["depth"] <= 31
@@ -246,8 +252,8 @@ def test_treelets_keep_results_and_cut_visits(rq, po):
     nrm = np.concatenate([Nn, np.zeros((n, 1))], 1).astype(np.float32)
     d = W.diag(V)
     rays = po.aorays(pos, nrm, np.zeros(n, np.float32), 1, 7, 1e-4 * d, 0.1 * d, 0.0)
-    plain = rq.HostBVH(V, I, rq.CWBVH, treelet_passes=-1)
-    opt = rq.HostBVH(V, I, rq.CWBVH)  # default passes
+    plain = rq.HostBVH(V, I, rq.CWBVH, treelet_passes=-1, spatial_splits=-1)
+    opt = rq.HostBVH(V, I, rq.CWBVH, spatial_splits=-1)  # default passes
     tr = opt.tree()
     assert np.array_equal(np.sort(tr["prim_refs"]), np.arange(I.shape[0]))
     assert tr["leaf_count"].max() <= 3
