@@ -17,7 +17,7 @@
 // Spatial-split budget (duplicate references, percent of the triangles) when
 // the caller asks for the default.
 #ifndef RQ_DEFAULT_SPATIAL_SPLITS
-#define RQ_DEFAULT_SPATIAL_SPLITS 100
+#define RQ_DEFAULT_SPATIAL_SPLITS 200
 #endif
 
 using namespace rq;

@@ -91,7 +91,7 @@ typedef struct rq_build_params {
                           /* before the 8-wide collapse (0 = default 4, negative = none)   */
     int spatial_splits;   /* binned spatial splits in the SAH build (as Embree's high-     */
                           /* quality builder): budget of duplicate triangle references in  */
-                          /* percent of the triangle count (0 = default 100, negative = none) */
+                          /* percent of the triangle count (0 = default 200, negative = none) */
 } rq_build_params;
 
 typedef struct rq_bvh_info {

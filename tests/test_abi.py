@@ -64,8 +64,8 @@ def test_host_build_and_info(rq):
     hb = rq.HostBVH(V, I, rq.CWBVH)
     info = hb.info
     assert info["node_float4s"] == 5 * info["node_count"]
-    # spatial splits (default budget 100 %) may store a triangle in several leaves
-    assert 3 * I.shape[0] <= info["woop_float4s"] <= 6 * I.shape[0]
+    # spatial splits (default budget 200 %) may store a triangle in several leaves
+    assert 3 * I.shape[0] <= info["woop_float4s"] <= 9 * I.shape[0]
     assert info["prim_index_count"] == info["woop_float4s"]
     assert np.allclose(info["bounds_lo"], V.min(0)) and np.allclose(info["bounds_hi"], V.max(0))
     once = rq.HostBVH(V, I, rq.CWBVH, spatial_splits=-1).info
