@@ -458,7 +458,31 @@ def main():
     # ---- the reference's CWBVH kernel rebuilt for sm_100a, same rays (closest-hit: its only mode)
     ref_gpu = None
     if not args.no_ref_gpu:
-        ref_gpu, _ = run_ref_gpu(scenes, rays, warmup=1, steps=2)
+        ref_gpu, ref_hits = run_ref_gpu(scenes, rays, warmup=1, steps=2)
+        if ref_hits and ref_gpu.get("value"):
+            # This library's closest-hit batch on the same rays: the like-for-like figure, and the
+            # closest triangles compared with the reference kernel's.
+            chits = [torch.empty_like(h) for h in hits]
+            cbatch = rq.Batch(ctx, [(ds.scene, r, h) for ds, r, h in zip(scenes, rays, chits)], rq.CLOSEST,
+                              params=bp)
+            ms_closest = time_steps(lambda: cbatch.run(stream), args.steps, warmup, stream, dist, flush)
+            ctx.check(stream)
+            same = total_n = 0
+            for ds, mine, theirs in zip(scenes, chits, ref_hits):
+                pm = torch.from_numpy(ds.host.prim_index).cuda()
+                a, b = mine[:, 1].view(torch.int32), theirs[:, 1].view(torch.int32)
+                pa = torch.where(a >= 0, pm[a.clamp(min=0).long()], torch.full_like(a, -1))
+                pb = torch.where(b >= 0, pm[b.clamp(min=0).long()], torch.full_like(b, -1))
+                same += int((pa == pb).sum().item())
+                total_n += int(a.numel())
+            ref_gpu["this_library_closest_hit"] = {
+                "value": round(total_rays / (ms_closest * 1e-3) / 1e6, 2), "unit": "Mrays/s",
+                "ms_per_step": round(ms_closest, 4), "launch": "one persistent batch, the any-hit autotuned shape",
+                "closest_prim_ids_equal_frac": round(same / max(total_n, 1), 6)}
+            ref_gpu["closest_vs_reference_kernel"] = round(total_rays / (ms_closest * 1e-3) / 1e6 / ref_gpu["value"],
+                                                          3)
+            cbatch.close()
+            del chits
 
     # ---- the plain config's per-kernel table: CWBVH and BVH2, any-hit and closest-hit, + the reference's BVH2
     kernels = None
@@ -778,7 +802,8 @@ def run_ref_gpu(scenes, rays, warmup: int, steps: int, kind: int = 0):
             "query": "closest-hit (the reference has no any-hit kernel)",
             "timing": f"sum of the reference's own CUDA-event kernel times (its log line per {tag} call)"
             if timed else f"host wall clock around synchronous {tag} calls",
-            "grid": "as shipped (CWBVH 32x32 blocks of 32x2 threads)"}, [h for h in out_hits]
+            "grid": "as shipped (CWBVH: 32x32 blocks of 32x2 threads; BVH2: one 128-thread block per 128 rays)"
+            }, [h for h in out_hits]
 
 
 def C_buffers(scene):
