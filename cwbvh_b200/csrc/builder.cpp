@@ -12,6 +12,7 @@
 // bin's box and centroid box, from which the children's bounds follow without
 // another pass; subtrees above a size threshold are built on other threads.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <future>
 #include <thread>
@@ -131,6 +132,15 @@ struct Builder2 {
         BBox box, cbox;
     };
 
+    // Threads for binning one large node; nodes below kParallelBin
+    // references are binned by the thread that builds them.
+    int threads_total = 1;
+    static constexpr int64_t kParallelBin = int64_t(1) << 20;
+    int64_t chunks_for(int64_t n) const {
+        if (threads_total <= 1 || n < kParallelBin) return 1;
+        return std::min<int64_t>(threads_total, n / (kParallelBin / 4));
+    }
+
     int32_t make_leaf(int64_t begin, int64_t end) {
         // Fragments of one split triangle can share a leaf: keep one of each.
         int64_t n = 0;
@@ -189,18 +199,40 @@ struct Builder2 {
         Bin(*bin)[kMaxBins] = reinterpret_cast<Bin(*)[kMaxBins]>(storage);
         for (int a = 0; a < 3; ++a)
             for (int i = 0; i < nb; ++i) new (&bin[a][i]) Bin();
-        for (int64_t k = begin; k < end; ++k) {
-            const PrimRef& p = refs[k];
-            float c[3];
-            centroid(p, c);
-            for (int a = 0; a < 3; ++a) {
-                int bi = (int)((c[a] - cb.lo[a]) * scale[a]);
-                bi = bi < 0 ? 0 : (bi >= nb ? nb - 1 : bi);
-                Bin& x = bin[a][bi];
-                x.count++;
-                x.box.grow(p.lo, p.hi);
-                x.cbox.grow_pt(c);
+        auto bin_refs = [&](int64_t k0, int64_t k1, Bin (*out)[kMaxBins]) {
+            for (int64_t k = k0; k < k1; ++k) {
+                const PrimRef& p = refs[k];
+                float c[3];
+                centroid(p, c);
+                for (int a = 0; a < 3; ++a) {
+                    int bi = (int)((c[a] - cb.lo[a]) * scale[a]);
+                    bi = bi < 0 ? 0 : (bi >= nb ? nb - 1 : bi);
+                    Bin& x = out[a][bi];
+                    x.count++;
+                    x.box.grow(p.lo, p.hi);
+                    x.cbox.grow_pt(c);
+                }
             }
+        };
+        const int64_t chunks = chunks_for(n);
+        if (chunks <= 1) {
+            bin_refs(begin, end, bin);
+        } else {
+            // Large nodes (the top of the tree, built before the subtrees
+            // spread over the threads): bin chunks in parallel, then merge;
+            // min/max and counts do not depend on the order.
+            std::vector<std::array<std::array<Bin, kMaxBins>, 3>> part((size_t)chunks);
+            parallel_tasks(chunks, threads_total, [&](int64_t c) {
+                Bin(*out)[kMaxBins] = reinterpret_cast<Bin(*)[kMaxBins]>(part[(size_t)c].data());
+                bin_refs(begin + n * c / chunks, begin + n * (c + 1) / chunks, out);
+            });
+            for (const auto& pc : part)
+                for (int a = 0; a < 3; ++a)
+                    for (int i = 0; i < nb; ++i) {
+                        bin[a][i].count += pc[(size_t)a][(size_t)i].count;
+                        bin[a][i].box.grow(pc[(size_t)a][(size_t)i].box);
+                        bin[a][i].cbox.grow(pc[(size_t)a][(size_t)i].cbox);
+                    }
         }
         float best_cost = INFINITY;
         int best_axis = -1, best_bin = -1;
@@ -306,22 +338,41 @@ struct Builder2 {
         SBin sbin[3][kMaxBins];
         bool usable[3];
         for (int a = 0; a < 3; ++a) usable[a] = b.hi[a] - b.lo[a] > 0.f;
-        for (int64_t k = begin; k < end; ++k) {
-            const PrimRef& r = refs[k];
-            BBox rbox;
-            rbox.grow(r.lo, r.hi);
-            for (int a = 0; a < 3; ++a) {
-                if (!usable[a]) continue;
-                const int b0 = bin_of(a, r.lo[a]), b1 = bin_of(a, r.hi[a]);
-                sbin[a][b0].enter++;
-                sbin[a][b1].exit++;
-                for (int j = b0; j <= b1; ++j) {
-                    BBox q = rbox;
-                    q.lo[a] = fmx(q.lo[a], plane(a, j));
-                    q.hi[a] = fmn(q.hi[a], plane(a, j + 1));
-                    sbin[a][j].box.grow(q);
+        auto bin_refs = [&](int64_t k0, int64_t k1, SBin (*out)[kMaxBins]) {
+            for (int64_t k = k0; k < k1; ++k) {
+                const PrimRef& r = refs[k];
+                BBox rbox;
+                rbox.grow(r.lo, r.hi);
+                for (int a = 0; a < 3; ++a) {
+                    if (!usable[a]) continue;
+                    const int b0 = bin_of(a, r.lo[a]), b1 = bin_of(a, r.hi[a]);
+                    out[a][b0].enter++;
+                    out[a][b1].exit++;
+                    for (int j = b0; j <= b1; ++j) {
+                        BBox q = rbox;
+                        q.lo[a] = fmx(q.lo[a], plane(a, j));
+                        q.hi[a] = fmn(q.hi[a], plane(a, j + 1));
+                        out[a][j].box.grow(q);
+                    }
                 }
             }
+        };
+        const int64_t chunks = chunks_for(n);
+        if (chunks <= 1) {
+            bin_refs(begin, end, sbin);
+        } else {
+            std::vector<std::array<std::array<SBin, kMaxBins>, 3>> part((size_t)chunks);
+            parallel_tasks(chunks, threads_total, [&](int64_t c) {
+                SBin(*out)[kMaxBins] = reinterpret_cast<SBin(*)[kMaxBins]>(part[(size_t)c].data());
+                bin_refs(begin + n * c / chunks, begin + n * (c + 1) / chunks, out);
+            });
+            for (const auto& pc : part)
+                for (int a = 0; a < 3; ++a)
+                    for (int i = 0; i < nb; ++i) {
+                        sbin[a][i].enter += pc[(size_t)a][(size_t)i].enter;
+                        sbin[a][i].exit += pc[(size_t)a][(size_t)i].exit;
+                        sbin[a][i].box.grow(pc[(size_t)a][(size_t)i].box);
+                    }
         }
         for (int a = 0; a < 3; ++a) {
             if (!usable[a]) continue;
@@ -606,6 +657,7 @@ static void build_from_refs(std::vector<PrimRef> refs, const Mesh* mesh, float s
     b.max_depth = max_depth;
     if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     b.spare_threads = threads - 1;
+    b.threads_total = threads;
     b.refs = std::move(refs);
     const int64_t nt = (int64_t)b.refs.size();
     BBox all, call;
