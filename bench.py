@@ -467,18 +467,23 @@ def main():
                               params=bp)
             ms_closest = time_steps(lambda: cbatch.run(stream), args.steps, warmup, stream, dist, flush)
             ctx.check(stream)
-            same = total_n = 0
+            same = total_n = bad_mine = bad_ref = 0
             for ds, mine, theirs in zip(scenes, chits, ref_hits):
                 pm = torch.from_numpy(ds.host.prim_index).cuda()
+                n_pm = pm.numel()
                 a, b = mine[:, 1].view(torch.int32), theirs[:, 1].view(torch.int32)
-                pa = torch.where(a >= 0, pm[a.clamp(min=0).long()], torch.full_like(a, -1))
-                pb = torch.where(b >= 0, pm[b.clamp(min=0).long()], torch.full_like(b, -1))
+                # indices are clamped into the map; addresses outside it are counted, not looked up
+                bad_mine += int((a >= n_pm).sum().item())
+                bad_ref += int((b >= n_pm).sum().item())
+                pa = torch.where((a >= 0) & (a < n_pm), pm[a.clamp(0, n_pm - 1).long()], torch.full_like(a, -1))
+                pb = torch.where((b >= 0) & (b < n_pm), pm[b.clamp(0, n_pm - 1).long()], torch.full_like(b, -1))
                 same += int((pa == pb).sum().item())
                 total_n += int(a.numel())
             ref_gpu["this_library_closest_hit"] = {
                 "value": round(total_rays / (ms_closest * 1e-3) / 1e6, 2), "unit": "Mrays/s",
                 "ms_per_step": round(ms_closest, 4), "launch": "one persistent batch, the any-hit autotuned shape",
-                "closest_prim_ids_equal_frac": round(same / max(total_n, 1), 6)}
+                "closest_prim_ids_equal_frac": round(same / max(total_n, 1), 6),
+                "hit_addresses_outside_the_primitive_map": {"this_library": bad_mine, "reference": bad_ref}}
             ref_gpu["closest_vs_reference_kernel"] = round(total_rays / (ms_closest * 1e-3) / 1e6 / ref_gpu["value"],
                                                           3)
             cbatch.close()
@@ -960,7 +965,9 @@ def run_city(args, world, rank, dist):
             mine = ph[:, 1].view(torch.int32)
             theirs = ref_hits[0][:, 1].view(torch.int32)
             pm = torch.from_numpy(hb.prim_index).cuda()
-            pid = lambda a: torch.where(a >= 0, pm[a.clamp(min=0).long()], torch.full_like(a, -1))  # noqa: E731
+            n_pm = pm.numel()
+            pid = lambda a: torch.where((a >= 0) & (a < n_pm), pm[a.clamp(0, n_pm - 1).long()],  # noqa: E731
+                                        torch.full_like(a, -1))
             ref["closest_prim_ids_equal_frac"] = round(float((pid(mine) == pid(theirs)).float().mean().item()), 6)
     total = 2 * n
     ms_total = ms_prim + ms_gen + ms_ao
