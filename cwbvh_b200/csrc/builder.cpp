@@ -327,7 +327,7 @@ struct Builder2 {
                 planes[a][k] = k == 0 ? b.lo[a] : (k == nb ? b.hi[a] : b.lo[a] + ext * ((float)k / (float)nb));
             to_bin[a] = ext > 0.f ? (float)nb / ext : 0.f;
         }
-        auto plane = [&](int a, int k) { return planes[a][k]; };
+        auto plane = [&](int ax, int k) { return planes[ax][k]; };
         auto bin_of = [&](int a, float x) {
             int k = (int)((x - b.lo[a]) * to_bin[a]);
             k = k < 0 ? 0 : (k >= nb ? nb - 1 : k);
@@ -403,7 +403,7 @@ struct Builder2 {
 
         // Distribute: wholly left / right, or straddling (split or unsplit).
         const int a = best_axis;
-        const float pos = b.lo[a] + (b.hi[a] - b.lo[a]) * ((float)best_plane / (float)nb);
+        const float pos = planes[a][best_plane];
         std::vector<PrimRef> left, right, straddle;
         left.reserve((size_t)best_nl);
         right.reserve((size_t)best_nr);
@@ -464,7 +464,7 @@ struct Builder2 {
         bounds_of(begin, begin + nl, lb, lcb);
         bounds_of(begin + nl + sl, begin + nl + sl + nr, rb, rcb);
         code = make_inner(Range{begin, begin + nl, begin + nl + sl, lb, lcb},
-                                    Range{begin + nl + sl, begin + nl + sl + nr, cap, rb, rcb}, depth);
+                          Range{begin + nl + sl, begin + nl + sl + nr, cap, rb, rcb}, depth);
         return true;
     }
 
