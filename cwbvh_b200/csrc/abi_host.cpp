@@ -91,6 +91,14 @@ rq_status rq_build_bvh(const float* vertices, int64_t nv, const int32_t* indices
         if (kind == RQ_BVH_BVH2) {
             build_bvh2_tree(m, std::max(1, bp.max_leaf_size), bp.sah_bins, bp.max_depth, true, bp.threads, h->b.tree2,
                             bp.presplit, split_budget);
+            if (bp.treelet_passes > 0 && !h->b.tree2.root_is_leaf) {
+                // Restructuring may deepen the tree: keep it only within the
+                // depth limit (stacks of BVH2 kernels are sized by it).
+                Tree<2> plain = h->b.tree2;
+                treelet_optimize(h->b.tree2, bp.treelet_passes, bp.threads);
+                if (tree_depth2(h->b.tree2) > std::max(tree_depth2(plain), bp.max_depth + 1))
+                    h->b.tree2 = std::move(plain);
+            }
             convert_bvh2(h->b.tree2, m, h->b);
             h->b.depth = tree_depth2(h->b.tree2);
         } else {

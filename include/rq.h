@@ -87,8 +87,9 @@ typedef struct rq_build_params {
     int threads;          /* builder threads (0 = hardware concurrency)                    */
     int presplit;         /* 1, 2, 4 or 8: cut badly fitting triangles into up to this     */
                           /* many references with clipped boxes before the build (0 = 1)   */
-    int treelet_passes;   /* CWBVH: passes of SAH treelet restructuring of the binary tree */
-                          /* before the 8-wide collapse (0 = default 4, negative = none)   */
+    int treelet_passes;   /* passes of SAH treelet restructuring of the binary tree (CWBVH: */
+                          /* before the 8-wide collapse; BVH2: kept if the depth stays     */
+                          /* within max_depth) (0 = default 4, negative = none)            */
     int spatial_splits;   /* binned spatial splits in the SAH build (as Embree's high-     */
                           /* quality builder): budget of duplicate triangle references in  */
                           /* percent of the triangle count (0 = default 200, negative = none) */

@@ -334,3 +334,27 @@ def test_spatial_splits_independent_of_thread_count(rq):
         assert np.array_equal(a.prim_index, b.prim_index)
     with pytest.raises(rq.RQError, match="INVALID_ARG"):
         rq.HostBVH(V, I, rq.CWBVH, spatial_splits=1000)
+
+
+def test_bvh2_treelets_keep_results_within_depth(rq, po):
+    """BVH2 builds are restructured too, and the result is kept only while
+    the depth stays within the build's limit (31 levels by default, the
+    reference BVH2 kernel's stack); answers are unchanged."""
+    from cwbvh_b200 import workloads as W
+    from adjudicate import _explained, prim_ids
+    V, I = W.scene_of_size(3, 150_000)
+    rays = _ao_rays_numpy(po, V, I, 20000, 5)
+    plain = rq.HostBVH(V, I, rq.BVH2, treelet_passes=-1)
+    opt = rq.HostBVH(V, I, rq.BVH2)
+    assert opt.info["depth"] <= 31
+    for any_hit in (True, False):
+        ha, va, _ = po.trace(rq.BVH2, plain.nodes, plain.woop, rays, any_hit, counts=True)
+        hb, vb, _ = po.trace(rq.BVH2, opt.nodes, opt.woop, rays, any_hit, counts=True)
+        x, y = prim_ids(ha, plain.prim_index), prim_ids(hb, opt.prim_index)
+        assert np.array_equal(x >= 0, y >= 0)
+        if not any_hit:
+            bad = np.nonzero(x != y)[0]
+            assert all(_explained(po, rays[k], V, I, (int(x[k]), int(y[k]))) for k in bad), len(bad)
+        assert vb.mean() < va.mean()
+    shallow = rq.HostBVH(V, I, rq.BVH2, max_depth=20)
+    assert shallow.info["depth"] <= 21
