@@ -358,3 +358,15 @@ def test_bvh2_treelets_keep_results_within_depth(rq, po):
         assert vb.mean() < va.mean()
     shallow = rq.HostBVH(V, I, rq.BVH2, max_depth=20)
     assert shallow.info["depth"] <= 21
+
+
+def test_large_node_binning_independent_of_thread_count(rq):
+    """Nodes of over 1M references are binned on all threads and merged; the
+    tree (and so every byte of the scene) is the same as on one thread."""
+    from cwbvh_b200 import workloads as W
+    V, I = W.scene_of_size(21, 1_100_000)
+    a = rq.HostBVH(V, I, rq.CWBVH, threads=1)
+    b = rq.HostBVH(V, I, rq.CWBVH, threads=8)
+    assert np.array_equal(a.nodes.view(np.uint32), b.nodes.view(np.uint32))
+    assert np.array_equal(a.woop.view(np.uint32), b.woop.view(np.uint32))
+    assert np.array_equal(a.prim_index, b.prim_index)
