@@ -248,7 +248,9 @@ class HostBVH:
                 "root_is_leaf": bool(rl.value)}
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        # `lib` is None once the interpreter is tearing modules down; the
+        # process exit releases the handle then.
+        if getattr(self, "_h", None) and lib is not None:
             lib.rq_host_bvh_free(self._h)
             self._h = None
 
@@ -323,7 +325,9 @@ class Scene:
         return int(lib.rq_scene_bytes(self._h))
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        # `lib` is None once the interpreter is tearing modules down; the
+        # process exit releases the handle then.
+        if getattr(self, "_h", None) and lib is not None:
             lib.rq_scene_destroy(self._h)
             self._h = None
 
@@ -346,7 +350,9 @@ class Context:
         return int(lib.rq_ctx_check(self._h, _stream(stream)))
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        # `lib` is None once the interpreter is tearing modules down; the
+        # process exit releases the handle then.
+        if getattr(self, "_h", None) and lib is not None:
             lib.rq_ctx_destroy(self._h)
             self._h = None
 
@@ -407,7 +413,9 @@ class Tlas:
                 "map": f(mp, nr.value, C.c_int32)}
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        # `lib` is None once the interpreter is tearing modules down; the
+        # process exit releases the handle then.
+        if getattr(self, "_h", None) and lib is not None:
             lib.rq_tlas_destroy(self._h)
             self._h = None
 
@@ -577,7 +585,9 @@ class Batch:
         check(lib.rq_batch_run(self._h, _stream(stream)), "rq_batch_run")
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        # `lib` is None once the interpreter is tearing modules down; the
+        # process exit releases the handle then.
+        if getattr(self, "_h", None) and lib is not None:
             lib.rq_batch_destroy(self._h)
             self._h = None
 
@@ -658,7 +668,9 @@ class Server:
         return int(lib.rq_server_cancel(self._h, ticket))
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
+        # `lib` is None once the interpreter is tearing modules down; the
+        # process exit releases the handle then.
+        if getattr(self, "_h", None) and lib is not None:
             lib.rq_server_destroy(self._h)
             self._h = None
 
