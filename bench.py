@@ -1136,10 +1136,11 @@ def run_large(args, world, rank, dist):
     gpu_trees = {}
     with torch.cuda.stream(stream):
         ghits = torch.empty((n, 4), device="cuda")
-    for passes in (0, 2):
+    for method, passes in ((rq.GPU_BUILD_LBVH, 0), (rq.GPU_BUILD_LBVH, 2), (rq.GPU_BUILD_PLOC, 0),
+                           (rq.GPU_BUILD_PLOC, 2)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        gsc = rq.Scene.build_gpu(v, i, optimize_passes=passes, stream=stream)
+        gsc = rq.Scene.build_gpu(v, i, optimize_passes=passes, method=method, stream=stream)
         torch.cuda.synchronize()
         t_gpu_build = time.perf_counter() - t0
         ms_gpu_tree = time_steps(lambda: rq.trace(ctx, gsc, rays, ghits, rq.ANY, stream=stream), args.steps, warmup,
@@ -1147,7 +1148,8 @@ def run_large(args, world, rank, dist):
         ctx.check(stream)
         torch.cuda.synchronize()
         same = float(((ghits[:, 1].view(torch.int32) != -1) == (hits[:, 1].view(torch.int32) != -1)).float().mean())
-        gpu_trees[f"treelet_passes_{passes}"] = {"build_s": round(t_gpu_build, 3),
+        tag = "lbvh" if method == rq.GPU_BUILD_LBVH else "ploc"
+        gpu_trees[f"{tag}_treelet_passes_{passes}"] = {"build_s": round(t_gpu_build, 3),
                                                  "mrays_per_s": round(n / (ms_gpu_tree * 1e-3) / 1e6, 2),
                                                  "occlusion_same_frac": round(same, 6)}
         del gsc
@@ -1183,8 +1185,9 @@ def run_large(args, world, rank, dist):
                                            what="rq_trace_ao: per-surfel occluded counts in the trace epilogue, "
                                                 "no hit buffer (memset of the counts included)")},
         "gpu_built_tree": dict(gpu_trees, host_build_s=round(t_host_build, 2),
-                               what="rq_build_scene_gpu: Morton-ordered linear BVH, treelet restructuring passes, "
-                                    "collapsed to CWBVH on the device"),
+                               what="rq_build_scene_gpu: Morton-ordered radix tree (lbvh) or locally-ordered "
+                                    "clustering (ploc), treelet restructuring passes, collapsed to CWBVH on the "
+                                    "device"),
         "sorted_occlusion_identical": same, "fused_counts_identical": fused_same,
         "ao_occluded_fraction": round(occ, 4),
         "triangles": int(I.shape[0]), "scene_bytes": int(hb.nodes.nbytes + hb.woop.nbytes),

@@ -20,8 +20,11 @@ import numpy as np
 from . import _native as N
 from ._native import ANY, BVH2, CLOSEST, CWBVH, Launch, RQError, check, lib
 
+GPU_BUILD_LBVH = 0  # rq_build_scene_gpu: Karras radix tree over the Morton order
+GPU_BUILD_PLOC = 1  # rq_build_scene_gpu: parallel locally-ordered clustering
+
 __all__ = [
-    "ANY", "BVH2", "CLOSEST", "CWBVH", "Launch", "RQError", "HostBVH", "Scene", "Context", "Batch", "Server",
+    "ANY", "BVH2", "CLOSEST", "CWBVH", "GPU_BUILD_LBVH", "GPU_BUILD_PLOC", "Launch", "RQError", "HostBVH", "Scene", "Context", "Batch", "Server",
     "trace", "trace_ordered", "trace_counted", "aorays", "sample_surfels", "ao_reduce", "sort_rays",
     "autotune", "autotune_batch", "default_launch", "woopify", "gen_heightfield_boxes", "gen_city",
     "gen_spheres_terrain", "rtBindCWBVHData", "rtTraceCWBVH", "rtBindBVH2Data", "rtTraceBVH2",
@@ -286,12 +289,16 @@ class Scene:
         return cls(h, kind)
 
     @classmethod
-    def build_gpu(cls, vertices, indices, optimize_passes: int = 2, stream=None) -> "Scene":
+    def build_gpu(cls, vertices, indices, optimize_passes: int = 2, method: int = GPU_BUILD_PLOC,
+                  stream=None) -> "Scene":
         """CWBVH built on the device (rq_build_scene_gpu) from CUDA tensors
-        vertices (nv, 3) float32 and indices (nt, 3) int32."""
+        vertices (nv, 3) float32 and indices (nt, 3) int32; `method` is
+        GPU_BUILD_PLOC (clustering, better trees) or GPU_BUILD_LBVH (radix
+        tree, fastest build)."""
         h = C.c_void_p()
         check(lib.rq_build_scene_gpu(_ptr(vertices), _rows(vertices, 3, "vertices"), _ptr(indices),
-                                     _rows(indices, 3, "indices"), optimize_passes, C.byref(h), _stream(stream)),
+                                     _rows(indices, 3, "indices"), method, optimize_passes, C.byref(h),
+                                     _stream(stream)),
               "rq_build_scene_gpu")
         return cls(h, CWBVH)
 

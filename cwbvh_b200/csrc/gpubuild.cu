@@ -24,6 +24,7 @@
 // The tree is a valid CWBVH for every trace kernel; it is not the host
 // builder's (no SAH), so traversal is slower and the bytes differ.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cfloat>
@@ -586,14 +587,198 @@ __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, in
 
 unsigned blocks_of(int64_t n, int b) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
 
+// ---- PLOC: parallel locally-ordered clustering (Meister and Bittner,
+// "Parallel Locally-Ordered Clustering for Bounding Volume Hierarchy
+// Construction", IEEE TVCG 2018).  The clusters start as the triangles in
+// Morton order; each round every cluster finds, among the kPlocRadius
+// clusters on either side of it, the one whose merged box has the least
+// surface area, mutual nearest neighbours merge into a new node (placed at
+// the lower position), and the array is compacted.  Merged boxes group
+// primitives by extent as well as position, which the Morton order alone
+// does not.  Node numbers come from prefix sums, counting down from n - 2 in
+// position order, so the last merge is the root (node 0) and the tree does
+// not depend on thread scheduling.
+constexpr int kPlocRadius = 16;
+
+struct CBox {
+    float lo[3], hi[3];
+};
+
+__device__ inline float merged_area(const CBox& a, const CBox& b) {
+    float lo[3], hi[3];
+    for (int q = 0; q < 3; ++q) {
+        lo[q] = fminf(a.lo[q], b.lo[q]);
+        hi[q] = fmaxf(a.hi[q], b.hi[q]);
+    }
+    return half_area(lo, hi);
+}
+
+__global__ void ploc_init_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, const float* v, const int32_t* idx,
+                                 int32_t* code, CBox* box) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    code[p] = ~(int32_t)p;
+    tri_box(v, idx, key_tri(k, p, idx_mask), box[p].lo, box[p].hi);
+}
+
+// Nearest neighbour of each cluster within the radius (least merged area;
+// ties to the lower position, so the relation is the same seen from both).
+__global__ void ploc_nn_kernel(const CBox* box, int64_t m, int32_t* nn) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const CBox bi = box[i];
+    const int64_t j0 = i - kPlocRadius < 0 ? 0 : i - kPlocRadius;
+    const int64_t j1 = i + kPlocRadius >= m ? m - 1 : i + kPlocRadius;
+    float best = FLT_MAX;
+    int64_t bj = i == 0 ? 1 : i - 1;
+    for (int64_t j = j0; j <= j1; ++j) {
+        if (j == i) continue;
+        const float d = merged_area(bi, box[j]);
+        if (d < best) { best = d; bj = j; }  // ascending j: the first minimum is the lowest position
+    }
+    nn[i] = (int32_t)bj;
+}
+
+// merge[i] = 1 for the lower cluster of a mutual pair; keep[i] = 0 for the
+// upper one (it is absorbed).  Both arrays have an extra zero at m for the
+// scans' totals.
+__global__ void ploc_flags_kernel(const int32_t* nn, int64_t m, int32_t* merge, int32_t* keep) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > m) return;
+    if (i == m) {
+        merge[i] = 0;
+        keep[i] = 0;
+        return;
+    }
+    const int32_t j = nn[i];
+    const bool mutual = nn[j] == (int32_t)i;
+    merge[i] = mutual && (int32_t)i < j;
+    keep[i] = !(mutual && (int32_t)i > j);
+}
+
+__global__ void ploc_merge_kernel(const int32_t* nn, const int32_t* merge, const int32_t* rank, int64_t m, int64_t top,
+                                  const uint64_t* k, uint64_t idx_mask, const float* v, const int32_t* idx,
+                                  int32_t* code, CBox* box, BNode* nodes, int32_t* leaf_parent) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !merge[i]) return;
+    const int32_t j = nn[i];
+    const int32_t node = (int32_t)(top - rank[i]);
+    const int32_t c[2] = {code[i], code[j]};
+    float clo[2][3], chi[2][3], cc[2];
+    int32_t cn[2];
+    for (int q = 0; q < 2; ++q) child_box(nodes, k, idx_mask, v, idx, c[q], clo[q], chi[q], cn[q], &cc[q]);
+    BNode& nd = nodes[node];
+    nd.left = c[0];
+    nd.right = c[1];
+    nd.parent = -1;
+    nd.count = cn[0] + cn[1];
+    CBox u;
+    for (int a = 0; a < 3; ++a) {
+        u.lo[a] = fminf(clo[0][a], clo[1][a]);
+        u.hi[a] = fmaxf(chi[0][a], chi[1][a]);
+        nd.lo[a] = u.lo[a];
+        nd.hi[a] = u.hi[a];
+    }
+    nd.cost = kCt * half_area(u.lo, u.hi) + cc[0] + cc[1];
+    for (int q = 0; q < 2; ++q) {
+        if (c[q] >= 0) nodes[c[q]].parent = node;
+        else leaf_parent[~c[q]] = node;
+    }
+    code[i] = node;
+    box[i] = u;
+}
+
+__global__ void ploc_compact_kernel(const int32_t* keep, const int32_t* pos, int64_t m, const int32_t* code,
+                                    const CBox* box, int32_t* code2, CBox* box2) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !keep[i]) return;
+    code2[pos[i]] = code[i];
+    box2[pos[i]] = box[i];
+}
+
 }  // namespace
 }  // namespace rq
 
 using namespace rq;
 
+// PLOC rounds on the clusters of the sorted triangles: nodes, boxes, counts,
+// costs and parent links as the radix tree + bottom-up boxes give them.
+static rq_status ploc_tree(const uint64_t* keys_sorted, uint64_t idx_mask, int64_t n, const float* vertices,
+                           const int32_t* indices, BNode* bn, int32_t* leaf_parent, cudaStream_t s) {
+    int32_t *code = nullptr, *code2 = nullptr, *nn = nullptr, *merge = nullptr, *keep = nullptr, *rank = nullptr,
+            *pos = nullptr;
+    CBox *box = nullptr, *box2 = nullptr;
+    void* temp = nullptr;
+    size_t temp_bytes = 0;
+    rq_status st = RQ_OK;
+    auto ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == RQ_OK) st = cuda_fail(e, "rq_build_scene_gpu (PLOC)");
+        return st == RQ_OK;
+    };
+    const int64_t n1 = n + 1;
+    if (ok(cudaMalloc(&code, n * sizeof(int32_t))) && ok(cudaMalloc(&code2, n * sizeof(int32_t))) &&
+        ok(cudaMalloc(&nn, n * sizeof(int32_t))) && ok(cudaMalloc(&merge, n1 * sizeof(int32_t))) &&
+        ok(cudaMalloc(&keep, n1 * sizeof(int32_t))) && ok(cudaMalloc(&rank, n1 * sizeof(int32_t))) &&
+        ok(cudaMalloc(&pos, n1 * sizeof(int32_t))) && ok(cudaMalloc(&box, n * sizeof(CBox))) &&
+        ok(cudaMalloc(&box2, n * sizeof(CBox))) &&
+        ok(cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, merge, rank, (int)n1, s)) &&
+        ok(cudaMalloc(&temp, std::max<size_t>(temp_bytes, 1)))) {
+        ploc_init_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, code, box);
+        ok(cudaGetLastError());
+        int64_t m = n, top = n - 2;
+        // Each round merges at least the globally closest pair in reach; a
+        // round that merges nothing (non-finite boxes) is an error.
+        for (int round = 0; st == RQ_OK && m > 1; ++round) {
+            if (round > 100000) {
+                st = RQ_ERR_BAD_SCENE;
+                break;
+            }
+            ploc_nn_kernel<<<blocks_of(m, 256), 256, 0, s>>>(box, m, nn);
+            ploc_flags_kernel<<<blocks_of(m + 1, 256), 256, 0, s>>>(nn, m, merge, keep);
+            ok(cudaGetLastError());
+            size_t tb = temp_bytes;
+            ok(cub::DeviceScan::ExclusiveSum(temp, tb, merge, rank, (int)(m + 1), s));
+            tb = temp_bytes;
+            ok(cub::DeviceScan::ExclusiveSum(temp, tb, keep, pos, (int)(m + 1), s));
+            int32_t totals[2] = {0, 0};
+            ok(cudaMemcpyAsync(&totals[0], rank + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            ok(cudaMemcpyAsync(&totals[1], pos + m, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            ok(cudaStreamSynchronize(s));
+            if (st != RQ_OK) break;
+            const int64_t merges = totals[0], kept = totals[1];
+            if (merges <= 0 || kept != m - merges || top - merges + 1 < 0) {
+                st = RQ_ERR_BAD_SCENE;
+                break;
+            }
+            ploc_merge_kernel<<<blocks_of(m, 256), 256, 0, s>>>(nn, merge, rank, m, top, keys_sorted, idx_mask,
+                                                                vertices, indices, code, box, bn, leaf_parent);
+            ploc_compact_kernel<<<blocks_of(m, 256), 256, 0, s>>>(keep, pos, m, code, box, code2, box2);
+            ok(cudaGetLastError());
+            std::swap(code, code2);
+            std::swap(box, box2);
+            top -= merges;
+            m = kept;
+        }
+        if (st == RQ_OK && top != -1) st = RQ_ERR_BAD_SCENE;  // n - 1 nodes, the root last (node 0)
+    }
+    ok(cudaStreamSynchronize(s));
+    cudaFree(code);
+    cudaFree(code2);
+    cudaFree(nn);
+    cudaFree(merge);
+    cudaFree(keep);
+    cudaFree(rank);
+    cudaFree(pos);
+    cudaFree(box);
+    cudaFree(box2);
+    cudaFree(temp);
+    return st;
+}
+
 extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt,
-                                        int optimize_passes, rq_scene_t* out, void* stream) {
+                                        int method, int optimize_passes, rq_scene_t* out, void* stream) {
     if (!out || !vertices || !indices || nv <= 0 || nt <= 0 || nt > (int64_t)INT32_MAX / 4) return RQ_ERR_INVALID_ARG;
+    if (method != RQ_GPU_BUILD_LBVH && method != RQ_GPU_BUILD_PLOC) return RQ_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t n = nt;
     // device scratch
@@ -662,10 +847,14 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
     }
     int64_t levels = 0, n_nodes = 1;
     if (st == RQ_OK && n > 1) {
-        radix_tree_kernel<<<blocks_of(n - 1, 256), 256, 0, s>>>(keys_sorted, n, bn, leaf_parent);
-        boxes_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn, leaf_parent,
-                                                       arrivals);
-        ok(cudaGetLastError(), "rq_build_scene_gpu");
+        if (method == RQ_GPU_BUILD_PLOC) {
+            st = ploc_tree(keys_sorted, idx_mask, n, vertices, indices, bn, leaf_parent, s);
+        } else {
+            radix_tree_kernel<<<blocks_of(n - 1, 256), 256, 0, s>>>(keys_sorted, n, bn, leaf_parent);
+            boxes_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,
+                                                           leaf_parent, arrivals);
+            ok(cudaGetLastError(), "rq_build_scene_gpu");
+        }
         for (int pass = 0; pass < optimize_passes && st == RQ_OK; ++pass) {
             ok(cudaMemsetAsync(arrivals, 0, (n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
             treelet_kernel<<<blocks_of(n, 128), 128, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,

@@ -17,12 +17,14 @@ def _device_mesh(V, I):
         torch.from_numpy(np.ascontiguousarray(I, np.int32)).cuda()
 
 
-@pytest.fixture(scope="module", params=[0, 2], ids=["linear", "treelets"])
+@pytest.fixture(scope="module", params=[(0, 0), (0, 2), (1, 0), (1, 2)],
+                ids=["lbvh", "lbvh-treelets", "ploc", "ploc-treelets"])
 def built(rq, request):
     from cwbvh_b200 import workloads as W
     V, I = W.scene_of_size(3, 150_000)
     v, i = _device_mesh(V, I)
-    sc = rq.Scene.build_gpu(v, i, optimize_passes=request.param)
+    method, passes = request.param
+    sc = rq.Scene.build_gpu(v, i, optimize_passes=passes, method=method)
     nodes, woop, prim = sc.download()
     return V, I, v, i, sc, nodes, woop, prim
 
@@ -72,9 +74,11 @@ def test_kernels_and_oracle_agree_on_gpu_tree(rq, po, built, query):
 def test_small_and_invalid_meshes(rq, po):
     import torch
     V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1]], np.float32)
-    for I in (np.array([[0, 1, 2]], np.int32), np.array([[0, 1, 2], [1, 3, 4]], np.int32)):
+    cases = [(I, method) for I in (np.array([[0, 1, 2]], np.int32), np.array([[0, 1, 2], [1, 3, 4]], np.int32))
+             for method in (rq.GPU_BUILD_LBVH, rq.GPU_BUILD_PLOC)]
+    for I, method in cases:
         v, i = _device_mesh(V, I)
-        sc = rq.Scene.build_gpu(v, i)
+        sc = rq.Scene.build_gpu(v, i, method=method)
         nodes, woop, prim = sc.download()
         rays = np.zeros((64, 8), np.float32)
         rays[:, 0:3] = [0.2, 0.2, -1.0]
@@ -88,5 +92,9 @@ def test_small_and_invalid_meshes(rq, po):
         assert np.array_equal(hits.cpu().numpy().view(np.uint32), want.view(np.uint32))
         assert (prim_ids(want, prim) == 0).all()  # the z = 0 triangle
     v, i = _device_mesh(V, np.array([[0, 1, 5]], np.int32))
+    for method in (rq.GPU_BUILD_LBVH, rq.GPU_BUILD_PLOC):
+        with pytest.raises(rq.RQError, match="INVALID_ARG"):
+            rq.Scene.build_gpu(v, i, method=method)
+    v, i = _device_mesh(V, np.array([[0, 1, 2]], np.int32))
     with pytest.raises(rq.RQError, match="INVALID_ARG"):
-        rq.Scene.build_gpu(v, i)
+        rq.Scene.build_gpu(v, i, method=7)
