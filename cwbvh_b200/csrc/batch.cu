@@ -230,6 +230,15 @@ static void cache_store(const char* path, const std::string& key, const rq_launc
       << l.fetch_nd << " " << l.fetch_nw << "\n";
 }
 
+// Second tuning stage: the refill thresholds (Nd, Nw; Nd -1 stands for 0)
+// and, for CWBVH, the triangle postponing ratio, tried on the launch shape
+// the first stage chose.
+struct FetchChoice {
+    int nd, nw;
+};
+constexpr FetchChoice kFetchChoices[] = {{2, 8}, {4, 4}, {1, 16}, {-1, 1}};
+constexpr float kRatioChoices[] = {0.2f, 0.3f};
+
 }  // namespace rq
 
 extern "C" {
@@ -276,6 +285,34 @@ rq_status rq_autotune(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit
                     best.postpone_ratio = rt < 0.f ? -1.0f : rt;
                 }
             }
+    if (st == RQ_OK) {
+        const rq_launch shape = best;
+        for (const FetchChoice& fc : kFetchChoices)
+            for (float rt : kRatioChoices) {
+                if (st != RQ_OK) break;
+                rq_launch l = shape;
+                l.fetch_nd = fc.nd;
+                l.fetch_nw = fc.nw;
+                if (scene->kind == RQ_BVH_CWBVH && shape.postpone_ratio > 0.f) l.postpone_ratio = rt;
+                else if (rt != kRatioChoices[0]) continue;  // the ratio does not apply
+                float ms_runs[3];
+                for (int r = 0; r < 4 && st == RQ_OK; ++r) {
+                    cudaEventRecord(e0, s);
+                    st = rq_trace(ctx, scene, rays, hits, count, query, &l, s);
+                    cudaEventRecord(e1, s);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (r > 0) ms_runs[r - 1] = ms;
+                }
+                if (st != RQ_OK) break;
+                std::sort(ms_runs, ms_runs + 3);
+                if (ms_runs[1] < best_ms) {
+                    best_ms = ms_runs[1];
+                    best = l;
+                }
+            }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != RQ_OK) return st;
@@ -364,6 +401,39 @@ rq_status rq_autotune_batch(rq_ctx_t ctx, const rq_batch_item* items, int n_item
                     best = bp;
                 }
             }
+    if (st == RQ_OK) {
+        const rq_batch_params shape = best;
+        const bool cw = items[0].scene->kind == RQ_BVH_CWBVH;
+        for (const FetchChoice& fc : kFetchChoices)
+            for (float rt : kRatioChoices) {
+                if (st != RQ_OK) break;
+                if (!cw && rt != kRatioChoices[0]) continue;  // no triangle postponing in BVH2
+                rq_batch_params bp = shape;
+                bp.launch.fetch_nd = fc.nd;
+                bp.launch.fetch_nw = fc.nw;
+                if (cw) bp.launch.postpone_ratio = rt;
+                rq_batch_t b = nullptr;
+                st = rq_batch_create(ctx, items, n_items, query, &bp, &b);
+                if (st != RQ_OK) break;
+                float ms_runs[2];
+                for (int r = 0; r < 3 && st == RQ_OK; ++r) {
+                    cudaEventRecord(e0, s);
+                    st = rq_batch_run(b, s);
+                    cudaEventRecord(e1, s);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (r > 0) ms_runs[r - 1] = ms;
+                }
+                rq_batch_destroy(b);
+                if (st != RQ_OK) break;
+                const float ms = std::min(ms_runs[0], ms_runs[1]);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = bp;
+                }
+            }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != RQ_OK) return st;

@@ -64,8 +64,9 @@ typedef struct rq_launch {
     int blocks_per_sm;    /* persistent grid = SMs x this (0 = occupancy max)   */
     int smem_stack;       /* stack entries per lane in shared memory: 4, 8, 16  */
     float postpone_ratio; /* triangle postponing threshold Rt (reference 0.2)   */
-    int fetch_nd;         /* dynamic fetch: idle lanes tolerated (default 0, reference 4)       */
-    int fetch_nw;         /* dynamic fetch: lost-iteration budget (default 1, reference 16)     */
+    int fetch_nd;         /* dynamic fetch: idle lanes tolerated per iteration (default 2,      */
+                          /* reference 4; negative = 0)                                          */
+    int fetch_nw;         /* dynamic fetch: lost-lane budget before a refill (default 8, ref. 16) */
     int step_limit;       /* node visits per ray before it ends with RQ_ERR_TIMEOUT (0 = 2^22) */
 } rq_launch;
 
@@ -322,18 +323,21 @@ rq_status rq_batch_destroy(rq_batch_t batch);
 
 /* ---------------------------------------------------------------- autotune */
 /*
- * Time the candidate launch shapes (block size, blocks per SM, shared-memory
- * stack depth, postponing ratio) on the given rays and return the fastest.
- * When cache_path is non-null the choice is stored there keyed by device,
- * BVH kind, query and size class, and later calls read it back.
+ * Time the candidate launch shapes (block size, shared-memory stack depth,
+ * postponing on/off) on the given rays, then, on the fastest shape, the
+ * dynamic-fetch refill thresholds (fetch_nd, fetch_nw) and the postponing
+ * ratio, and return the fastest.  When cache_path is non-null the choice is
+ * stored there keyed by device, BVH kind, query and size class, and later
+ * calls read it back.
  */
 rq_status rq_autotune(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,
                       int64_t count, rq_query query, const char* cache_path, rq_launch* out,
                       void* stream);
 
 /* Tune a whole batch: sort threshold (never / large items / all) x block size
- * x shared-memory stack depth, timed on the batch itself, cached like
- * rq_autotune.  use_graph is set when `stream` is not the default stream. */
+ * x shared-memory stack depth, then refill thresholds and postponing ratio on
+ * the fastest of those, timed on the batch itself, cached like rq_autotune.
+ * use_graph is set when `stream` is not the default stream. */
 rq_status rq_autotune_batch(rq_ctx_t ctx, const rq_batch_item* items, int n_items, rq_query query,
                             const char* cache_path, rq_batch_params* out, void* stream);
 
