@@ -117,8 +117,23 @@ def test_autotune_returns_valid_launch(rq, batch_set, tmp_path):
     cache = str(tmp_path / "tune.txt")
     l = rq.autotune(ctx, ds.scene, rays, hits, rq.ANY, cache_path=cache)
     assert l.block_size in (64, 128, 256) and l.smem_stack in (4, 8, 16)
+    # second stage: refill thresholds from the candidates (Nd -1 stands for 0)
+    fetch = {(2, 8), (4, 4), (1, 16), (-1, 1)}
+    assert (l.fetch_nd, l.fetch_nw) in fetch
     l2 = rq.autotune(ctx, ds.scene, rays, hits, rq.ANY, cache_path=cache)  # from the cache
-    assert (l2.block_size, l2.smem_stack) == (l.block_size, l.smem_stack)
+    fields = ("block_size", "smem_stack", "postpone_ratio", "fetch_nd", "fetch_nw")
+    assert [getattr(l2, f) for f in fields] == [getattr(l, f) for f in fields]
     items = [(d.scene, r, torch.empty((r.shape[0], 4), device="cuda")) for (_, _, d, r) in batch_set]
     bp = rq.autotune_batch(ctx, items, rq.ANY, cache_path=cache, stream=torch.cuda.Stream())
     assert bp.launch.block_size in (64, 128, 256) and bp.use_graph == 1
+    assert (bp.launch.fetch_nd, bp.launch.fetch_nw) in fetch
+    assert min(abs(bp.launch.postpone_ratio - r) for r in (0.2, 0.3)) < 1e-6
+    bp2 = rq.autotune_batch(ctx, items, rq.ANY, cache_path=cache, stream=torch.cuda.Stream())
+    assert [getattr(bp2.launch, f) for f in fields] == [getattr(bp.launch, f) for f in fields]
+    assert (bp2.sort_threshold, bp2.use_graph) == (bp.sort_threshold, bp.use_graph)
+    # the tuned launch traces to the same occlusion as the defaults
+    a, b = torch.empty_like(hits), torch.empty_like(hits)
+    rq.trace(ctx, ds.scene, rays, a, rq.ANY)
+    rq.trace(ctx, ds.scene, rays, b, rq.ANY, launch=l)
+    ctx.check()
+    assert torch.equal(a[:, 1].view(torch.int32) != -1, b[:, 1].view(torch.int32) != -1)
