@@ -370,3 +370,31 @@ def test_large_node_binning_independent_of_thread_count(rq):
     assert np.array_equal(a.nodes.view(np.uint32), b.nodes.view(np.uint32))
     assert np.array_equal(a.woop.view(np.uint32), b.woop.view(np.uint32))
     assert np.array_equal(a.prim_index, b.prim_index)
+
+
+def test_spatial_splits_with_degenerate_triangles(rq, po):
+    """Zero-area (point and collinear) and duplicated triangles mixed into a
+    mesh: the spatial-split build stays valid and answers as the plain build."""
+    from cwbvh_b200 import workloads as W
+    from adjudicate import prim_ids
+    V, I = W.heightfield_boxes(2, grid=24, n_boxes=30)
+    rng = np.random.default_rng(3)
+    k = 400
+    pts = rng.uniform(0, 1, (k, 3)).astype(np.float32)
+    base = V.shape[0]
+    line = np.concatenate([pts, pts + np.float32(0.05), pts + np.float32(0.1)])  # collinear triples
+    V2 = np.concatenate([V, pts, line]).astype(np.float32)
+    point_tris = np.stack([base + np.arange(k)] * 3, 1)
+    col = base + k + np.arange(k)
+    line_tris = np.stack([col, col + k, col + 2 * k], 1)
+    dup = I[rng.integers(0, I.shape[0], 200)]
+    I2 = np.concatenate([I, point_tris, line_tris, dup]).astype(np.int32)
+    rays = _ao_rays_numpy(po, V, I, 10000, 4)
+    plain = rq.HostBVH(V2, I2, rq.CWBVH, spatial_splits=-1)
+    split = rq.HostBVH(V2, I2, rq.CWBVH, spatial_splits=200)
+    tr = split.tree()
+    assert np.array_equal(np.unique(tr["prim_refs"]), np.arange(I2.shape[0]))
+    for any_hit in (True, False):
+        a = prim_ids(po.trace(0, plain.nodes, plain.woop, rays, any_hit), plain.prim_index)
+        b = prim_ids(po.trace(0, split.nodes, split.woop, rays, any_hit), split.prim_index)
+        assert np.array_equal(a >= 0, b >= 0)
