@@ -45,17 +45,20 @@ def log(*a):
 # --------------------------------------------------------------- workload --
 
 def workload_spec(name: str, quick: bool, rank: int):
+    """Scenes are the same on every rank (scene seed = item index) and every
+    rank traces its own rays (ray seed per rank), so the replicas do equal
+    host work and take the same code paths."""
+    from cwbvh_b200.replicas import rank_seed
     rng = np.random.default_rng(12345)
     if name == "small":
-        return [dict(seed=0, tris=10592, rays=1 << 20, small=True)]
+        return [dict(seed=0, ray_seed=rank_seed(0, rank) + 1000, tris=10592, rays=1 << 20, small=True)]
     n = 64 if not quick else 8
     tris = np.exp(rng.uniform(math.log(10_000), math.log(2_000_000), 64)).astype(np.int64)[:n]
     rays = np.exp(rng.uniform(math.log(256 * 1024), math.log(8 * 1024 * 1024), 64)).astype(np.int64)[:n]
     if quick:
         tris = np.minimum(tris, 200_000)
         rays = np.minimum(rays, 1 << 20)
-    from cwbvh_b200.replicas import rank_seed
-    return [dict(seed=rank_seed(i, rank), tris=int(t), rays=int(r), small=False)
+    return [dict(seed=i, ray_seed=rank_seed(i, rank) + 1000, tris=int(t), rays=int(r), small=False)
             for i, (t, r) in enumerate(zip(tris, rays))]
 
 
@@ -68,7 +71,9 @@ def build_scenes(spec, threads_per_build: int = 1):
         hb = rq.HostBVH(V, I, rq.CWBVH, threads=threads_per_build)
         return V, I, hb
 
-    workers = max(1, min(len(spec), (os.cpu_count() or 1)))
+    # ranks on one node share its cores
+    ranks_here = max(1, int(os.environ.get("LOCAL_WORLD_SIZE", "1")))
+    workers = max(1, min(len(spec), (os.cpu_count() or 1) // ranks_here))
     with cf.ThreadPoolExecutor(max_workers=workers) as ex:
         return list(ex.map(one, spec))
 
@@ -335,7 +340,7 @@ def main():
             sc = rq.Scene.from_host(hb)
             ds = W.DeviceScene(rq.CWBVH, hb, sc, torch.from_numpy(V).cuda(), torch.from_numpy(I).cuda(),
                                W.diag(V), I.shape[0])
-            r = W.ao_rays(ds, s["rays"], seed=s["seed"] + 1000, stream=stream)
+            r = W.ao_rays(ds, s["rays"], seed=s["ray_seed"], stream=stream)
             scenes.append(ds)
             rays.append(r)
             hits.append(torch.empty((s["rays"], 4), device="cuda"))
@@ -456,8 +461,9 @@ def main():
     link_ms = link_bound_ms(total_rays * 32, total_rays * 16, link)
 
     # ---- the reference's CWBVH kernel rebuilt for sm_100a, same rays (closest-hit: its only mode)
+    # (at N = 1 only, like the serving and CPU baselines below: reference figures, not the scaled value)
     ref_gpu = None
-    if not args.no_ref_gpu:
+    if not args.no_ref_gpu and world == 1:
         ref_gpu, ref_hits = run_ref_gpu(scenes, rays, warmup=1, steps=2)
         if ref_hits and ref_gpu.get("value"):
             # This library's closest-hit batch on the same rays: the like-for-like figure, and the
@@ -496,7 +502,7 @@ def main():
 
     # ---- serving configuration (continuous batching vs one request per launch)
     serving = None
-    if not args.no_serving and args.workload == "batched" and not args.quick:
+    if not args.no_serving and args.workload == "batched" and not args.quick and world == 1:
         del host_rays, host_hits
         torch.cuda.empty_cache()
         t0 = time.time()
@@ -505,7 +511,7 @@ def main():
 
     # ---- CPU baseline (oracle restatement, all host threads, bounded sample)
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(spec, built)
 
     world_rays = total_rays * world
