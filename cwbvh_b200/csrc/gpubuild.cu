@@ -429,10 +429,82 @@ __device__ inline float area(const float lo[3], const float hi[3]) {
 }
 
 // Expands the binary nodes of one level into 8-wide nodes.
+// ---- Cost-optimal collapse into 8-wide nodes (the host builder's dynamic
+// programme): for every binary node and k = 1..8 slots, the least
+// surface-area cost of representing its subtree with at most k children of
+// an 8-wide node -- one leaf (at most 3 triangles), an 8-wide node of its
+// own, or the node opened with j slots to its left child and k - j to its
+// right.  Computed bottom-up (the second child to finish completes a node);
+// the expansion then replays the choices instead of opening the largest
+// child greedily.
+constexpr float kCollapseNode = 1.0f;  // per 8-wide node, times its area
+constexpr float kCollapseLeaf = 0.3f;  // per triangle in a leaf, times the leaf's area
+
+struct CollapseDP {
+    float best[8];    // k = 1..8
+    uint8_t how[8];   // 0 leaf, 1 own node, 2 + j opened with j slots to the left child
+    uint8_t split8;   // slots to the left child when the node is an 8-wide node of its own
+    uint8_t pad[7];
+};
+
+__global__ void collapse_dp_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, const float* v,
+                                   const int32_t* idx, const BNode* nodes, const int32_t* leaf_parent,
+                                   int32_t* arrivals, CollapseDP* dp) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int32_t node = leaf_parent[p];
+    while (node >= 0) {
+        __threadfence();
+        if (atomicAdd(&arrivals[node], 1) == 0) return;  // the sibling finishes this node
+        __threadfence();
+        const int32_t c[2] = {__ldcg(&nodes[node].left), __ldcg(&nodes[node].right)};
+        float cost[2][9], area[2];
+        int32_t cnt[2];
+        for (int q = 0; q < 2; ++q) {
+            float lo[3], hi[3];
+            child_box(nodes, k, idx_mask, v, idx, c[q], lo, hi, cnt[q]);
+            area[q] = half_area(lo, hi);
+            for (int kk = 1; kk <= 8; ++kk)
+                cost[q][kk] = c[q] >= 0 ? __ldcg(&dp[c[q]].best[kk - 1]) : kCollapseLeaf * area[q];
+        }
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = __ldcg(&nodes[node].lo[a]);
+            hi[a] = __ldcg(&nodes[node].hi[a]);
+        }
+        const float av = half_area(lo, hi);
+        const int32_t prims = cnt[0] + cnt[1];
+        float open[9];
+        uint8_t split[9];
+        for (int kk = 2; kk <= 8; ++kk) {
+            open[kk] = FLT_MAX;
+            split[kk] = 1;
+            for (int j = 1; j < kk; ++j) {
+                const float cc = cost[0][j] + cost[1][kk - j];
+                if (cc < open[kk]) { open[kk] = cc; split[kk] = (uint8_t)j; }
+            }
+        }
+        CollapseDP d;
+        const float as_node = kCollapseNode * av + open[8];
+        const float as_leaf = prims <= 3 ? kCollapseLeaf * av * (float)prims : FLT_MAX;
+        d.best[0] = fminf(as_leaf, as_node);
+        d.how[0] = as_leaf <= as_node ? 0 : 1;
+        for (int kk = 2; kk <= 8; ++kk) {
+            d.best[kk - 1] = d.best[kk - 2];
+            d.how[kk - 1] = d.how[kk - 2];
+            if (open[kk] < d.best[kk - 1]) { d.best[kk - 1] = open[kk]; d.how[kk - 1] = (uint8_t)(2 + split[kk]); }
+        }
+        d.split8 = split[8];
+        dp[node] = d;
+        node = __ldcg(&nodes[node].parent);
+    }
+}
+
 __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, int64_t next_cap, const BNode* nodes,
                               const uint64_t* k, uint64_t idx_mask, const float* v, const int32_t* idx,
                               float4* out_nodes,
-                              int64_t node_cap, float4* woop, int32_t* prim, int64_t tri_cap, Ctr* ctr) {
+                              int64_t node_cap, float4* woop, int32_t* prim, int64_t tri_cap, Ctr* ctr,
+                              const CollapseDP* dp) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n_items) return;
     const Item it = items[w];
@@ -444,6 +516,38 @@ __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, in
         code[0] = it.code;
         child_box(nodes, k, idx_mask, v, idx, it.code, clo[0], chi[0], cnt[0]);
         m = 1;
+    } else if (dp) {
+        // the slots the collapse chose: (binary child, slots it fills), left first
+        int32_t stc[16];
+        int stk[16];
+        int sp = 0;
+        const BNode& b = nodes[it.code];
+        const int s8 = dp[it.code].split8;
+        stc[sp] = b.right; stk[sp++] = 8 - s8;
+        stc[sp] = b.left; stk[sp++] = s8;
+        while (sp > 0) {
+            --sp;
+            const int32_t x = stc[sp];
+            const int kk = stk[sp];
+            const int h = (x >= 0 && kk >= 1 && kk <= 8) ? dp[x].how[kk - 1] : 0;
+            if (h >= 2) {
+                const int j = h - 2;
+                if (sp + 2 > 16 || j < 1 || j >= kk) {  // a table the recursion cannot follow
+                    atomicOr(&ctr->error, 4u);
+                    return;
+                }
+                stc[sp] = nodes[x].right; stk[sp++] = kk - j;
+                stc[sp] = nodes[x].left; stk[sp++] = j;
+            } else {
+                if (m >= 8) {
+                    atomicOr(&ctr->error, 4u);
+                    return;
+                }
+                code[m] = x;
+                child_box(nodes, k, idx_mask, v, idx, x, clo[m], chi[m], cnt[m]);
+                ++m;
+            }
+        }
     } else {
         const BNode& b = nodes[it.code];
         code[0] = b.left;
@@ -785,6 +889,7 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
     uint64_t *keys = nullptr, *keys_sorted = nullptr;
     BNode* bn = nullptr;
     int32_t *leaf_parent = nullptr, *arrivals = nullptr;
+    CollapseDP* dp = nullptr;
     unsigned* ob = nullptr;
     Item *qa = nullptr, *qb = nullptr;
     Ctr* ctr = nullptr;
@@ -810,6 +915,7 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
         ok(cudaMalloc(&bn, std::max<int64_t>(1, n - 1) * sizeof(BNode)), "rq_build_scene_gpu") &&
         ok(cudaMalloc(&leaf_parent, n * sizeof(int32_t)), "rq_build_scene_gpu") &&
         ok(cudaMalloc(&arrivals, std::max<int64_t>(1, n - 1) * sizeof(int32_t)), "rq_build_scene_gpu") &&
+        ok(cudaMalloc(&dp, std::max<int64_t>(1, n - 1) * sizeof(CollapseDP)), "rq_build_scene_gpu") &&
         ok(cudaMalloc(&ob, 6 * sizeof(unsigned)), "rq_build_scene_gpu") &&
         ok(cudaMalloc(&qa, q_cap * sizeof(Item)), "rq_build_scene_gpu") &&
         ok(cudaMalloc(&qb, q_cap * sizeof(Item)), "rq_build_scene_gpu") &&
@@ -861,6 +967,12 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
                                                              leaf_parent, arrivals, kTreeletLeaves);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
         }
+        if (st == RQ_OK) {
+            ok(cudaMemsetAsync(arrivals, 0, (n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
+            collapse_dp_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,
+                                                                 leaf_parent, arrivals, dp);
+            ok(cudaGetLastError(), "rq_build_scene_gpu");
+        }
     }
     if (st == RQ_OK) {
         // level 0: the root (binary node 0, or the single triangle)
@@ -872,7 +984,7 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
         while (st == RQ_OK && n_items > 0) {
             expand_kernel<<<blocks_of(n_items, 128), 128, 0, s>>>(qa, n_items, qb, q_cap, bn, keys_sorted, idx_mask,
                                                                   vertices, indices, nodes, node_cap, woop, prim, n,
-                                                                  ctr);
+                                                                  ctr, n > 1 ? dp : nullptr);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
             Ctr c{};
             ok(cudaMemcpyAsync(&c, ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, s), "rq_build_scene_gpu");
@@ -896,6 +1008,7 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
     cudaFree(bn);
     cudaFree(leaf_parent);
     cudaFree(arrivals);
+    cudaFree(dp);
     cudaFree(ob);
     cudaFree(qa);
     cudaFree(qb);
