@@ -935,7 +935,7 @@ def run_city(args, world, rank, dist):
     look = (float(0.5 * (lo[0] + hi[0])), float(0.5 * (lo[1] + hi[1])), 0.0)
     w = h = 2048 if args.quick else 4096
     n = w * h
-    prim = rq.camera_rays(eye, look, (0.0, 0.0, 1.0), 60.0, w, h, 0.0, 10.0 * dg, stream=stream)
+    prim = rq.camera_rays(eye, look, (0.0, 0.0, 1.0), 60.0, w, h, 0.0, 10.0 * dg, stream=stream, tile=(4, 8))
     with torch.cuda.stream(stream):
         ph = torch.empty((n, 4), device="cuda")
     ms_prim = time_steps(lambda: rq.trace(ctx, sc, prim, ph, rq.CLOSEST, stream=stream), args.steps, warmup,
@@ -994,7 +994,8 @@ def run_city(args, world, rank, dist):
     if ref:
         extra["reference_cwbvh_kernel_sm100a_primary"] = ref
     line = _single_line(args, world, warmup, f"city: {I.shape[0]/1e6:.2f}M tris, {w}x{h} primary closest-hit "
-                        "+ 1 AO any-hit ray per primary hit (tmax 0.05 diag); value = both passes + raygen",
+                        "(camera rays in 4x8-pixel tiles) + 1 AO any-hit ray per primary hit (tmax 0.05 diag); "
+                        "value = both passes + raygen",
                         world * total / (ms_total * 1e-3) / 1e6, ms_total, extra)
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -1051,7 +1052,7 @@ def run_instanced(args, world, rank, dist):
     look = (float(0.5 * (lo[0] + hi[0])), float(0.5 * (lo[1] + hi[1])), 0.0)
     w = h = 2048 if args.quick else 4096
     n = w * h
-    prim = rq.camera_rays(eye, look, (0.0, 0.0, 1.0), 60.0, w, h, 0.0, 10.0 * dg, stream=stream)
+    prim = rq.camera_rays(eye, look, (0.0, 0.0, 1.0), 60.0, w, h, 0.0, 10.0 * dg, stream=stream, tile=(4, 8))
     with torch.cuda.stream(stream):
         fh = torch.empty((n, 4), device="cuda")
         ih = torch.empty((n, 4), device="cuda")
@@ -1088,8 +1089,8 @@ def run_instanced(args, world, rank, dist):
         "instances": n_inst, "templates": len(templates), "flat_triangles": int(FI.shape[0]), "image": f"{w}x{h}",
     }
     line = _single_line(args, world, warmup, f"instanced city: {n_inst} instances of {len(templates)} 16-building "
-                        f"blocks ({FI.shape[0]/1e6:.2f}M tris flattened), {w}x{h} primary closest-hit + 1 AO any-hit "
-                        "ray per pixel; value = both instanced passes", world * 2 * n / (total_ms * 1e-3) / 1e6,
+                        f"blocks ({FI.shape[0]/1e6:.2f}M tris flattened), {w}x{h} primary closest-hit (4x8-pixel tiles) "
+                        "+ 1 AO any-hit ray per pixel; value = both instanced passes", world * 2 * n / (total_ms * 1e-3) / 1e6,
                         total_ms, extra)
     if rank == 0:
         print(json.dumps(line), flush=True)

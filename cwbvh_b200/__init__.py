@@ -521,14 +521,19 @@ def sample_surfels(vertices, indices, n: int, seed: int = 0, stream=None):
 
 
 def camera_rays(eye, look, up, vfov_deg: float, width: int, height: int, tmin: float = 0.0, tmax: float = 1e20,
-                stream=None):
-    """Pinhole camera rays, one per pixel, row-major (a torch CUDA (w*h, 8) tensor)."""
+                stream=None, tile: Optional[tuple] = None):
+    """Pinhole camera rays, one per pixel (a torch CUDA (w*h, 8) tensor):
+    row-major, or with tile=(tw, th) in tile order (rq_camera_rays_tiled)."""
     import torch
     with _On(stream):
         out = torch.empty((width * height, 8), dtype=torch.float32, device="cuda")
     f3 = lambda v: (C.c_float * 3)(*[float(x) for x in v])  # noqa: E731
-    check(lib.rq_camera_rays(f3(eye), f3(look), f3(up), vfov_deg, width, height, tmin, tmax, _ptr(out),
-                             _stream(stream)), "rq_camera_rays")
+    if tile is None:
+        check(lib.rq_camera_rays(f3(eye), f3(look), f3(up), vfov_deg, width, height, tmin, tmax, _ptr(out),
+                                 _stream(stream)), "rq_camera_rays")
+    else:
+        check(lib.rq_camera_rays_tiled(f3(eye), f3(look), f3(up), vfov_deg, width, height, int(tile[0]),
+                                       int(tile[1]), tmin, tmax, _ptr(out), _stream(stream)), "rq_camera_rays_tiled")
     return out
 
 

@@ -149,6 +149,7 @@ _sig("rq_scene_sizes", C.c_int, vp, P(i64), P(i64), P(i64))
 # rays and AO
 _sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)
 _sig("rq_camera_rays", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, f32, f32, vp, vp)
+_sig("rq_camera_rays_tiled", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, C.c_int, C.c_int, f32, f32, vp, vp)
 _sig("rq_surfels_from_hits", C.c_int, vp, vp, vp, i64, vp, vp, vp, vp)
 _sig("rq_probe_l2_read", C.c_int, vp, i64, C.c_int, vp, vp)
 _sig("rq_trace_ao", C.c_int, vp, vp, vp, i64, C.c_int, vp, P(Launch), vp)

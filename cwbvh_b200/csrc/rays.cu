@@ -111,11 +111,19 @@ __global__ void surfels_kernel(const float* __restrict__ v, const int32_t* __res
 }
 
 // Pinhole camera: pixel (x, y) centre through an image plane at distance 1.
+// Ray i is pixel (x, y) of tile i / (tw * th), tiles row-major across the
+// image and pixels row-major within a tile (tw = width, th = 1: the image
+// row-major).
 __global__ void camera_rays_kernel(float3 eye, float3 fwd, float3 right, float3 upv, float half_w, float half_h,
-                                   int width, int height, float tmin, float tmax, Ray* __restrict__ out) {
+                                   int width, int height, int tw, int th, float tmin, float tmax,
+                                   Ray* __restrict__ out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int64_t)width * height) return;
-    const int x = (int)(i % width), y = (int)(i / width);
+    const int64_t tile = i / ((int64_t)tw * th);
+    const int in_tile = (int)(i % ((int64_t)tw * th));
+    const int tiles_x = width / tw;
+    const int x = (int)(tile % tiles_x) * tw + in_tile % tw;
+    const int y = (int)(tile / tiles_x) * th + in_tile / tw;
     const float sx = ((x + 0.5f) / width * 2.0f - 1.0f) * half_w;
     const float sy = (1.0f - (y + 0.5f) / height * 2.0f) * half_h;
     const float3 d = norm3(add3(add3(fwd, mul3(right, sx)), mul3(upv, sy)));
@@ -318,10 +326,12 @@ rq_status rq_sample_surfels(const float* vertices, const int32_t* indices, int64
     return RQ_OK;
 }
 
-rq_status rq_camera_rays(const float eye[3], const float look[3], const float up[3], float vfov_deg, int width,
-                         int height, float tmin, float tmax, rq_ray* out_rays, void* stream) {
+static rq_status camera_rays_impl(const float eye[3], const float look[3], const float up[3], float vfov_deg,
+                                  int width, int height, int tw, int th, float tmin, float tmax, rq_ray* out_rays,
+                                  void* stream) {
     if (!eye || !look || !up || width <= 0 || height <= 0 || !(vfov_deg > 0.f && vfov_deg < 180.f) || !out_rays)
         return RQ_ERR_INVALID_ARG;
+    if (tw <= 0 || th <= 0 || width % tw != 0 || height % th != 0) return RQ_ERR_INVALID_ARG;
     // Camera frame on the host (once per call).
     auto norm = [](float3 a) {
         const float l = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
@@ -343,9 +353,21 @@ rq_status rq_camera_rays(const float eye[3], const float look[3], const float up
     const float half_w = half_h * (float)width / (float)height;
     const int64_t n = (int64_t)width * height;
     camera_rays_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(e, fwd, right, upv, half_w, half_h, width,
-                                                                             height, tmin, tmax, (Ray*)out_rays);
+                                                                             height, tw, th, tmin, tmax,
+                                                                             (Ray*)out_rays);
     RQ_CUDA(cudaGetLastError());
     return RQ_OK;
+}
+
+rq_status rq_camera_rays(const float eye[3], const float look[3], const float up[3], float vfov_deg, int width,
+                         int height, float tmin, float tmax, rq_ray* out_rays, void* stream) {
+    return camera_rays_impl(eye, look, up, vfov_deg, width, height, width, 1, tmin, tmax, out_rays, stream);
+}
+
+rq_status rq_camera_rays_tiled(const float eye[3], const float look[3], const float up[3], float vfov_deg,
+                               int width, int height, int tile_w, int tile_h, float tmin, float tmax,
+                               rq_ray* out_rays, void* stream) {
+    return camera_rays_impl(eye, look, up, vfov_deg, width, height, tile_w, tile_h, tmin, tmax, out_rays, stream);
 }
 
 rq_status rq_surfels_from_hits(const rq_scene* scene, const rq_ray* rays, const rq_hit* hits, int64_t count,

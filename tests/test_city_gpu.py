@@ -51,6 +51,24 @@ def test_camera_rays(rq):
     assert np.abs(rays[:, 4:7] - _camera_numpy(W_PX, H_PX, 50.0)).max() < 2e-6
 
 
+def test_camera_rays_tiled(rq):
+    """Tile order is a permutation of the row-major rays, bit for bit."""
+    import torch
+    rows = rq.camera_rays(EYE, LOOK, UP, 50.0, W_PX, H_PX, tmin=0.0, tmax=1e4)
+    tw, th = 4, 8
+    tiled = rq.camera_rays(EYE, LOOK, UP, 50.0, W_PX, H_PX, tmin=0.0, tmax=1e4, tile=(tw, th))
+    i = np.arange(W_PX * H_PX)
+    tile, r = i // (tw * th), i % (tw * th)
+    x = (tile % (W_PX // tw)) * tw + r % tw
+    y = (tile // (W_PX // tw)) * th + r // tw
+    pix = torch.from_numpy(y * W_PX + x).cuda()
+    assert torch.equal(tiled.view(torch.int32), rows[pix].view(torch.int32))
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        rq.camera_rays(EYE, LOOK, UP, 50.0, W_PX, H_PX, tile=(5, 8))  # 192 is not a multiple of 5
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        rq.camera_rays(EYE, LOOK, UP, 50.0, W_PX, H_PX, tile=(0, 8))
+
+
 def test_camera_rays_bad_args(rq):
     with pytest.raises(rq.RQError):
         rq.camera_rays(EYE, EYE, UP, 50.0, 8, 8)  # look == eye
