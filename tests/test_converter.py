@@ -398,3 +398,46 @@ def test_spatial_splits_with_degenerate_triangles(rq, po):
         a = prim_ids(po.trace(0, plain.nodes, plain.woop, rays, any_hit), plain.prim_index)
         b = prim_ids(po.trace(0, split.nodes, split.woop, rays, any_hit), split.prim_index)
         assert np.array_equal(a >= 0, b >= 0)
+
+
+@pytest.mark.parametrize("case", ["soup", "slivers", "tiny", "huge", "coplanar"])
+def test_build_options_keep_answers_on_random_meshes(rq, po, case):
+    """Spatial splits and treelet restructuring change only the tree: on
+    random triangle soups (thin slivers, coordinates near 1e-4 and 1e4, a
+    coplanar grid) every ray gets the same occlusion bit and closest
+    triangle (up to FP64-explained ties and edges) as the plain SAH build."""
+    from adjudicate import _explained, prim_ids
+    rng = np.random.default_rng(["soup", "slivers", "tiny", "huge", "coplanar"].index(case) + 11)
+    n = 3000
+    if case == "coplanar":
+        g = 40
+        x, y = np.meshgrid(np.arange(g + 1), np.arange(g + 1))
+        V = np.stack([x.ravel(), y.ravel(), np.zeros(x.size)], 1).astype(np.float32) / g
+        q = (np.arange(g)[:, None] * (g + 1) + np.arange(g)[None, :]).ravel()
+        I = np.concatenate([np.stack([q, q + 1, q + g + 2], 1), np.stack([q, q + g + 2, q + g + 1], 1)]).astype(np.int32)
+    else:
+        c = rng.uniform(0, 1, (n, 3))
+        e = rng.normal(size=(n, 2, 3)) * (0.02 if case != "slivers" else np.array([0.002, 0.002, 0.3]))
+        V = np.concatenate([c, c + e[:, 0], c + e[:, 1]]).astype(np.float64)
+        I = np.stack([np.arange(n), n + np.arange(n), 2 * n + np.arange(n)], 1).astype(np.int32)
+        scale = {"tiny": 1e-4, "huge": 1e4}.get(case, 1.0)
+        V = (V * scale).astype(np.float32)
+    lo, hi = V.min(0), V.max(0)
+    m = 8000
+    rays = np.zeros((m, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(lo - 0.1 * (hi - lo), hi + 0.1 * (hi - lo), (m, 3))
+    d = rng.normal(size=(m, 3))
+    if case == "coplanar":
+        rays[:, 2] = 0.5
+        d[:, 2] = -np.abs(d[:, 2]) - 0.2
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 3] = 0.0
+    rays[:, 7] = float(np.linalg.norm(hi - lo)) * 2
+    plain = rq.HostBVH(V, I, rq.CWBVH, spatial_splits=-1, treelet_passes=-1)
+    opt = rq.HostBVH(V, I, rq.CWBVH)
+    for any_hit in (True, False):
+        a = prim_ids(po.trace(0, plain.nodes, plain.woop, rays, any_hit), plain.prim_index)
+        b = prim_ids(po.trace(0, opt.nodes, opt.woop, rays, any_hit), opt.prim_index)
+        bad = np.nonzero((a >= 0) != (b >= 0))[0] if any_hit else np.nonzero(a != b)[0]
+        assert all(_explained(po, rays[k], V, I, (int(a[k]), int(b[k]))) for k in bad), (case, any_hit, len(bad))
+        assert (b >= 0).mean() > 0.05
