@@ -1,28 +1,32 @@
 // CWBVH built on the GPU from device-resident triangles, for scenes that must
 // be ready quickly (a new scene admitted into a server) rather than traced
-// at the best speed: a linear BVH (Morton-ordered triangles, Karras's radix
-// tree, bottom-up boxes) collapsed top-down into 8-wide nodes written
-// directly in the CWBVH node format, with Woop rows and the primitive map,
-// all on one stream.
+// at the best speed: a binary BVH over the Morton-ordered triangles (Karras's
+// radix tree, or locally-ordered clustering), optional treelet passes, then
+// a cost-optimal collapse into 8-wide nodes written directly in the CWBVH
+// node format, with Woop rows and the primitive map, all on one stream.
 //
 //  1. centroid bounds (reduction), Morton code of each centroid above the
 //     triangle number (unique 64-bit keys: ceil(log2 n) index bits, the rest,
 //     up to 21 per axis, for the code), radix sort;
-//  2. internal node i of the binary radix tree over the sorted keys: its key
-//     range and split from the longest common prefixes (Karras, "Maximizing
-//     Parallelism in the Construction of BVHs, Octrees, and k-d Trees",
-//     HPG 2012), parent links;
-//  3. boxes and triangle counts bottom-up: each leaf walks to the root and
-//     the second thread to reach a node completes it (one atomic per node);
-//  4. level by level from the root: a binary node that becomes an 8-wide
-//     node opens its largest child until it has 8 children; children with at
-//     most 3 triangles become leaves, the others 8-wide nodes of the next
-//     level.  Slots are assigned by the same octant rule as the host
-//     converter, boxes quantized the same way, inner children get one
-//     contiguous block and leaf triangles one contiguous run per node.
+//  2. the binary tree: either internal node i of the radix tree over the
+//     sorted keys, its key range and split from the longest common prefixes
+//     (Karras, "Maximizing Parallelism in the Construction of BVHs, Octrees,
+//     and k-d Trees", HPG 2012), with boxes and triangle counts bottom-up
+//     (each leaf walks to the root and the second thread to reach a node
+//     completes it, one atomic per node); or rounds of locally-ordered
+//     clustering (see ploc_tree);
+//  3. optional treelet restructuring passes (see restructure);
+//  4. the host builder's cost-optimal collapse (dynamic programme over 1..8
+//     slots per binary node, bottom-up), then level by level from the root
+//     each 8-wide node's slots as it chose them; children with at most 3
+//     triangles become leaves, the others 8-wide nodes of the next level.
+//     Slots are assigned by the same octant rule as the host converter,
+//     boxes quantized the same way, inner children get one contiguous block
+//     and leaf triangles one contiguous run per node.
 //
 // The tree is a valid CWBVH for every trace kernel; it is not the host
-// builder's (no SAH), so traversal is slower and the bytes differ.
+// builder's (no spatial splits, different binary tree), so traversal is
+// slower and the bytes differ.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -423,12 +427,6 @@ struct Ctr {
     unsigned int error;
 };
 
-__device__ inline float area(const float lo[3], const float hi[3]) {
-    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
-    return dx * dy + dy * dz + dz * dx;
-}
-
-// Expands the binary nodes of one level into 8-wide nodes.
 // ---- Cost-optimal collapse into 8-wide nodes (the host builder's dynamic
 // programme): for every binary node and k = 1..8 slots, the least
 // surface-area cost of representing its subtree with at most k children of
@@ -500,6 +498,8 @@ __global__ void collapse_dp_kernel(const uint64_t* k, uint64_t idx_mask, int64_t
     }
 }
 
+// Expands the binary nodes of one level into 8-wide nodes, their slots as
+// the collapse chose them.
 __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, int64_t next_cap, const BNode* nodes,
                               const uint64_t* k, uint64_t idx_mask, const float* v, const int32_t* idx,
                               float4* out_nodes,
@@ -549,27 +549,8 @@ __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, in
             }
         }
     } else {
-        const BNode& b = nodes[it.code];
-        code[0] = b.left;
-        code[1] = b.right;
-        child_box(nodes, k, idx_mask, v, idx, b.left, clo[0], chi[0], cnt[0]);
-        child_box(nodes, k, idx_mask, v, idx, b.right, clo[1], chi[1], cnt[1]);
-        m = 2;
-        // open the largest child that would become an 8-wide node, while slots remain
-        while (m < 8) {
-            int best = -1;
-            float ba = -1.f;
-            for (int c = 0; c < m; ++c)
-                if (code[c] >= 0 && cnt[c] > 3 && area(clo[c], chi[c]) > ba) { ba = area(clo[c], chi[c]); best = c; }
-            if (best < 0) break;
-            const BNode& o = nodes[code[best]];
-            const int32_t l = o.left, r = o.right;
-            code[best] = l;
-            child_box(nodes, k, idx_mask, v, idx, l, clo[best], chi[best], cnt[best]);
-            code[m] = r;
-            child_box(nodes, k, idx_mask, v, idx, r, clo[m], chi[m], cnt[m]);
-            ++m;
-        }
+        atomicOr(&ctr->error, 4u);  // an inner node needs the collapse table
+        return;
     }
     // node box
     float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
