@@ -3,7 +3,6 @@ the mix; requests arriving while others run are admitted and overlap; failures
 (unknown scene, over-budget request, cancellation, shutdown) come back as
 status codes."""
 import threading
-import time
 
 import numpy as np
 import pytest
@@ -55,7 +54,17 @@ def test_results_same_alone_and_in_mix(rq, scenes):
         st = srv.wait(t)
         assert st["status"] == 0
         alone.append(hits.copy())
-    # in the mix: all submitted at once from two threads, pageable and pinned buffers
+    # in the mix: the server's three streams are first kept busy by large
+    # requests (pageable hit buffers: their results come back after the
+    # stream's work), then all requests are submitted at once from two
+    # threads, pageable and pinned buffers, while those run
+    big = 3_000_000
+    blockers = []
+    for k in range(3):
+        br = _pinned((big, 8))
+        br[:] = _rays(W, scenes[1], big, 900 + k)
+        bh = np.zeros((big, 4), np.float32)
+        blockers.append((br, bh, srv.submit(ids[1], br, bh)))
     mix = [None] * len(reqs)
     tickets = [None] * len(reqs)
 
@@ -65,7 +74,6 @@ def test_results_same_alone_and_in_mix(rq, scenes):
             hits = np.zeros((rays.shape[0], 4), np.float32) if k % 2 else _pinned((rays.shape[0], 4))
             mix[k] = hits
             tickets[k] = srv.submit(ids[sid], rays, hits)
-            time.sleep(0.001)
 
     th = [threading.Thread(target=submitter, args=(range(j, len(reqs), 2),)) for j in range(2)]
     for t in th:
@@ -73,9 +81,11 @@ def test_results_same_alone_and_in_mix(rq, scenes):
     for t in th:
         t.join()
     stats = [srv.wait(t) for t in tickets]
+    for _, _, t in blockers:
+        assert srv.wait(t)["status"] == 0
     srv.close()
     batches = {s["batch_id"] for s in stats}
-    assert len(batches) < len(reqs)  # requests were gathered into shared launches
+    assert len(batches) < len(reqs)  # requests that arrived while others ran shared launches
     for k, (sid, rays) in enumerate(reqs):
         pi = scenes[sid].host.prim_index
         assert np.array_equal(prim_ids(alone[k], pi) >= 0, prim_ids(mix[k], pi) >= 0), k
