@@ -46,10 +46,17 @@ template <bool MULTI>
 __device__ __forceinline__ Ray fetch_ray(const TraceParams& p, int64_t g, Lane& L) {
     const TraceItem* it = &p.single;
     if (MULTI) {
-        int lo = 0, hi = p.n_items - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (p.items[mid].ray_begin <= g) lo = mid; else hi = mid - 1;
+        // A lane's rays come from a counter that only grows, so its next ray
+        // is in its current item or a later one: check the next item's start
+        // first, and search only forward when the ray lies beyond it.
+        int lo = L.item, hi = p.n_items - 1;
+        if (lo < 0 || lo > hi || p.items[lo].ray_begin > g) lo = 0;
+        if (lo < hi && p.items[lo + 1].ray_begin <= g) {
+            ++lo;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (p.items[mid].ray_begin <= g) lo = mid; else hi = mid - 1;
+            }
         }
         it = p.items + lo;
         L.item = lo;
