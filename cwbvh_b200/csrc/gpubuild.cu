@@ -706,8 +706,11 @@ __global__ void ploc_init_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n
     tri_box(v, idx, key_tri(k, p, idx_mask), box[p].lo, box[p].hi);
 }
 
-// Nearest neighbour of each cluster within the radius (least merged area;
-// ties to the lower position, so the relation is the same seen from both).
+// Nearest neighbour of each cluster within the radius: least merged area,
+// ties to the nearer position, then to the cluster's partner i ^ 1, then to
+// the lower position.  The rule is the same seen from both sides of a pair,
+// and clusters with identical boxes (duplicated geometry) pair off with
+// their partners, half of them merging per round instead of one pair.
 __global__ void ploc_nn_kernel(const CBox* box, int64_t m, int32_t* nn) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
@@ -715,11 +718,20 @@ __global__ void ploc_nn_kernel(const CBox* box, int64_t m, int32_t* nn) {
     const int64_t j0 = i - kPlocRadius < 0 ? 0 : i - kPlocRadius;
     const int64_t j1 = i + kPlocRadius >= m ? m - 1 : i + kPlocRadius;
     float best = FLT_MAX;
-    int64_t bj = i == 0 ? 1 : i - 1;
+    int64_t bj = i == 0 ? 1 : i - 1, bdist = INT64_MAX;
+    bool bpartner = false;
     for (int64_t j = j0; j <= j1; ++j) {
         if (j == i) continue;
         const float d = merged_area(bi, box[j]);
-        if (d < best) { best = d; bj = j; }  // ascending j: the first minimum is the lowest position
+        const int64_t dist = j > i ? j - i : i - j;
+        const bool partner = j == (i ^ 1);
+        // ascending j: among full ties the first is the lowest position
+        if (d < best || (d == best && (dist < bdist || (dist == bdist && partner && !bpartner)))) {
+            best = d;
+            bj = j;
+            bdist = dist;
+            bpartner = partner;
+        }
     }
     nn[i] = (int32_t)bj;
 }

@@ -98,3 +98,35 @@ def test_small_and_invalid_meshes(rq, po):
     v, i = _device_mesh(V, np.array([[0, 1, 2]], np.int32))
     with pytest.raises(rq.RQError, match="INVALID_ARG"):
         rq.Scene.build_gpu(v, i, method=7)
+
+
+def test_duplicated_geometry(rq, po):
+    """Many identical triangles (every box the same) besides a normal mesh:
+    both methods build promptly and trace as the oracle does on their trees;
+    every copy is stored."""
+    import time
+    import torch
+    from cwbvh_b200 import workloads as W
+    V, I = W.heightfield_boxes(4, grid=16, n_boxes=10)
+    dup = np.repeat(I[:1], 50_000, axis=0)
+    I2 = np.concatenate([I, dup]).astype(np.int32)
+    v, i = _device_mesh(V, I2)
+    rays = np.zeros((4096, 8), np.float32)
+    rng = np.random.default_rng(2)
+    rays[:, 0:3] = rng.uniform(-0.1, 1.1, (4096, 3))
+    d = rng.normal(size=(4096, 3))
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 7] = 3.0
+    for method in (rq.GPU_BUILD_LBVH, rq.GPU_BUILD_PLOC):
+        t0 = time.perf_counter()
+        sc = rq.Scene.build_gpu(v, i, method=method)
+        torch.cuda.synchronize()
+        assert time.perf_counter() - t0 < 20.0
+        nodes, woop, prim = sc.download()
+        assert np.array_equal(np.sort(prim.reshape(-1, 3)[:, 0]), np.arange(I2.shape[0]))
+        hits = torch.empty((4096, 4), device="cuda")
+        ctx = rq.Context()
+        rq.trace_ordered(ctx, sc, torch.from_numpy(rays).cuda(), hits, rq.CLOSEST)
+        ctx.check()
+        want = po.trace(rq.CWBVH, nodes, woop, rays, False)
+        assert np.array_equal(hits.cpu().numpy().view(np.uint32), want.view(np.uint32))
