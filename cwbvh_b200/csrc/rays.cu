@@ -370,7 +370,7 @@ rq_status rq_camera_rays_tiled(const float eye[3], const float look[3], const fl
     return camera_rays_impl(eye, look, up, vfov_deg, width, height, tile_w, tile_h, tmin, tmax, out_rays, stream);
 }
 
-rq_status rq_surfels_from_hits(const rq_scene* scene, const rq_ray* rays, const rq_hit* hits, int64_t count,
+rq_status rq_surfels_from_hits(rq_scene_t scene, const rq_ray* rays, const rq_hit* hits, int64_t count,
                                float* out_pos, float* out_nrm, float* out_radius, void* stream) {
     if (!scene || count < 0 || (count > 0 && (!rays || !hits || !out_pos || !out_nrm))) return RQ_ERR_INVALID_ARG;
     if (count == 0) return RQ_OK;

@@ -261,7 +261,7 @@ rq_status rq_camera_rays_tiled(const float eye[3], const float look[3], const fl
  * rq_aorays emits an empty ray (tmin = tmax = 0).  hits must come from a
  * closest-hit trace of this scene; a hit address outside its Woop buffer is
  * treated as a miss. */
-rq_status rq_surfels_from_hits(const rq_scene* scene, const rq_ray* rays, const rq_hit* hits,
+rq_status rq_surfels_from_hits(rq_scene_t scene, const rq_ray* rays, const rq_hit* hits,
                                int64_t count, float* out_pos, float* out_nrm, float* out_radius,
                                void* stream);
 

@@ -109,3 +109,38 @@ def test_no_device_errors_cleanly(rq):
     h = C.c_void_p()
     st = rq.lib.rq_ctx_create(C.byref(h))
     assert st in (5, 10)  # RQ_ERR_CUDA or RQ_ERR_NO_DEVICE
+
+
+def test_header_compiles_and_links_from_c(tmp_path):
+    """include/rq.h is plain C: a C11 program includes it with every warning
+    as an error, links against librq.so and runs the host-only entry points
+    (build a BVH over two triangles, read its info, free it)."""
+    import shutil
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "t.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "rq.h"
+int main(void) {
+    const float v[12] = {0, 0, 0, 1, 0, 0, 0, 1, 0, 1, 1, 0};
+    const int32_t idx[6] = {0, 1, 2, 1, 3, 2};
+    rq_host_bvh_t hb = NULL;
+    rq_build_params bp = {0};
+    bp.spatial_splits = -1;
+    if (rq_build_bvh(v, 4, idx, 2, RQ_BVH_CWBVH, &bp, &hb) != RQ_OK) return 1;
+    rq_bvh_info info;
+    if (rq_host_bvh_info(hb, &info) != RQ_OK) return 2;
+    printf("%lld %lld %s\n", (long long)info.node_count, (long long)info.woop_float4s, rq_status_string(RQ_OK));
+    rq_host_bvh_free(hb);
+    return info.woop_float4s == 6 ? 0 : 3;
+}
+''')
+    exe = tmp_path / "t"
+    inc = ROOT / "include"
+    subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-Werror", "-pedantic", f"-I{inc}", str(src), "-o", str(exe),
+                    str(LIB), f"-Wl,-rpath,{LIB.parent}"], check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    assert out.stdout.split()[-1] == "RQ_OK"
