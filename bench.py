@@ -49,12 +49,10 @@ def workload_spec(name: str, quick: bool, rank: int):
     rank traces its own rays (ray seed per rank), so the replicas do equal
     host work and take the same code paths."""
     from cwbvh_b200.replicas import rank_seed
-    rng = np.random.default_rng(12345)
+    from cwbvh_b200.workloads import batched_sizes
     if name == "small":
         return [dict(seed=0, ray_seed=rank_seed(0, rank) + 1000, tris=10592, rays=1 << 20, small=True)]
-    n = 64 if not quick else 8
-    tris = np.exp(rng.uniform(math.log(10_000), math.log(2_000_000), 64)).astype(np.int64)[:n]
-    rays = np.exp(rng.uniform(math.log(256 * 1024), math.log(8 * 1024 * 1024), 64)).astype(np.int64)[:n]
+    tris, rays = batched_sizes(64 if not quick else 8)
     if quick:
         tris = np.minimum(tris, 200_000)
         rays = np.minimum(rays, 1 << 20)

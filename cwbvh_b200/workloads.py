@@ -3,6 +3,7 @@ mesh.dat / samplecache.dat (src/main.cpp:29-77).
 
   heightfield_boxes   64x64 heightfield (8,192 tris) + 200 boxes (2,400 tris)
   scene_of_size       the same family scaled to a triangle count (batched sets)
+  batched_sizes       triangle and ray counts of the 64-scene batched workload
   city / large        the mid-size and large procedural scenes
   ao_rays             AO rays from surfels at uniform (triangle, barycentric)
                       points, cosine-weighted about the geometric normal,
@@ -66,3 +67,13 @@ def ao_rays(ds: DeviceScene, n_rays: int, seed: int, tmax_scale: float = 0.1, sp
 
 def log_uniform(rng: np.random.Generator, lo: float, hi: float, n: int) -> np.ndarray:
     return np.exp(rng.uniform(math.log(lo), math.log(hi), n))
+
+
+def batched_sizes(n: int = 64):
+    """The batched workload's (triangles, rays) per scene: 64 draws from
+    log-uniform [10k, 2M] triangles and [256K, 8M] rays (seed 12345), the
+    first n of them; 19.1M triangles and 126.7M rays over all 64."""
+    rng = np.random.default_rng(12345)
+    tris = np.exp(rng.uniform(math.log(10_000), math.log(2_000_000), 64)).astype(np.int64)[:n]
+    rays = np.exp(rng.uniform(math.log(256 * 1024), math.log(8 * 1024 * 1024), 64)).astype(np.int64)[:n]
+    return tris, rays
