@@ -290,15 +290,16 @@ class Scene:
 
     @classmethod
     def build_gpu(cls, vertices, indices, optimize_passes: int = 2, method: int = GPU_BUILD_PLOC,
-                  stream=None) -> "Scene":
+                  split_budget: int = 0, stream=None) -> "Scene":
         """CWBVH built on the device (rq_build_scene_gpu) from CUDA tensors
         vertices (nv, 3) float32 and indices (nt, 3) int32; `method` is
         GPU_BUILD_PLOC (clustering, better trees) or GPU_BUILD_LBVH (radix
-        tree, fastest build)."""
+        tree, fastest build); `split_budget` (percent of the triangles, 0 =
+        none) lets badly fitting triangles be cut into extra references."""
         h = C.c_void_p()
         check(lib.rq_build_scene_gpu(_ptr(vertices), _rows(vertices, 3, "vertices"), _ptr(indices),
-                                     _rows(indices, 3, "indices"), method, optimize_passes, C.byref(h),
-                                     _stream(stream)),
+                                     _rows(indices, 3, "indices"), method, optimize_passes, split_budget,
+                                     C.byref(h), _stream(stream)),
               "rq_build_scene_gpu")
         return cls(h, CWBVH)
 

@@ -144,7 +144,7 @@ _sig("rq_save_samplecache_dat", C.c_int, cp, i32, i32, vp, vp, vp)
 _sig("rq_free_host", None, vp)
 _sig("rq_host_bvh_save", C.c_int, vp, cp)
 _sig("rq_host_bvh_load", C.c_int, cp, P(vp))
-_sig("rq_build_scene_gpu", C.c_int, vp, i64, vp, i64, C.c_int, C.c_int, P(vp), vp)
+_sig("rq_build_scene_gpu", C.c_int, vp, i64, vp, i64, C.c_int, C.c_int, C.c_int, P(vp), vp)
 _sig("rq_scene_sizes", C.c_int, vp, P(i64), P(i64), P(i64))
 # rays and AO
 _sig("rq_sort_rays_static", C.c_int, vp, i64, vp, vp, vp, vp, vp)

@@ -28,6 +28,7 @@
 // builder's (no spatial splits, different binary tree), so traversal is
 // slower and the bytes differ.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -75,6 +76,247 @@ __device__ inline void tri_box(const float* v, const int32_t* idx, int64_t t, fl
 __global__ void check_indices_kernel(const int32_t* idx, int64_t n3, int64_t nv, unsigned* bad) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n3; q += (int64_t)gridDim.x * blockDim.x)
         if (idx[q] < 0 || (int64_t)idx[q] >= nv) atomicOr(bad, 1u);
+}
+
+// ---- Triangle pre-splitting (the splitting stage of Karras and Aila, "Fast
+// Parallel Construction of High-Quality Bounding Volume Hierarchies", HPG
+// 2013, section 5).  A triangle whose box is much larger than the triangle
+// itself (a sliver lying across the axes) is cut into several references
+// along the planes of a 1024^3 grid over the scene, the most important plane
+// first, so that the tree stages see tight boxes.  Each triangle receives
+// pieces in proportion to its priority (2^m * wasted area)^(1/3), where m is
+// the Morton level of the most important grid plane its box crosses and the
+// wasted area is its box's half area minus the least half area boxes of its
+// pieces can reach; the budget caps the extra pieces.  The references go to
+// the tree stages as a "box mesh": a reference with box [lo, hi] is the
+// triangle (lo, hi, hi), whose bounds are that box, so those stages read
+// reference boxes through the same code as triangle boxes.  Only the Woop
+// rows and the primitive map go back to the triangle.
+constexpr int kSplitGridBits = 10;
+constexpr int kMaxPieces = 32;
+
+struct SplitGrid {
+    float b0[3], ext[3];
+};
+
+__device__ inline SplitGrid split_grid(const unsigned* sb) {
+    SplitGrid g;
+    for (int a = 0; a < 3; ++a) {
+        g.b0[a] = ord2f(sb[a]);
+        g.ext[a] = ord2f(sb[3 + a]) - g.b0[a];
+    }
+    return g;
+}
+
+__device__ inline int grid_cell(const SplitGrid& g, int a, float x) {
+    const float f = (x - g.b0[a]) / g.ext[a] * (float)(1 << kSplitGridBits);
+    return (int)fminf(fmaxf(floorf(f), 0.f), (float)((1 << kSplitGridBits) - 1));
+}
+
+// The most important grid plane strictly inside [lo, hi]: the highest bit in
+// which the cells of lo and hi differ, x before y before z at equal bits (the
+// Morton order).  Returns its Morton level (3 * bit + 2 - axis) or -1.
+__device__ int split_plane(const SplitGrid& g, const float lo[3], const float hi[3], int& axis, float& pos) {
+    int best = -1;
+    for (int a = 0; a < 3; ++a) {
+        if (!(g.ext[a] > 0.f)) continue;
+        const int q0 = grid_cell(g, a, lo[a]), q1 = grid_cell(g, a, hi[a]);
+        if (q0 >= q1) continue;
+        const int bit = 31 - __clz(q0 ^ q1);
+        const int level = 3 * bit + 2 - a;
+        if (level <= best) continue;
+        const int cell = (q1 >> bit) << bit;  // first cell above the plane
+        const float p = g.b0[a] + g.ext[a] * ((float)cell / (float)(1 << kSplitGridBits));
+        if (!(p > lo[a] && p < hi[a])) continue;
+        best = level;
+        axis = a;
+        pos = p;
+    }
+    return best;
+}
+
+// Scene bounds of the triangle boxes as order-preserving unsigned min / max.
+__global__ void scene_bounds_kernel(const float* v, const int32_t* idx, int64_t n, unsigned* sb) {
+    unsigned mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t* ti = idx + 3 * t;
+        for (int c = 0; c < 3; ++c) {
+            const float3 p = vtx(v, ti[c]);
+            const unsigned u[3] = {f2ord(p.x), f2ord(p.y), f2ord(p.z)};
+            for (int a = 0; a < 3; ++a) {
+                mn[a] = min(mn[a], u[a]);
+                mx[a] = max(mx[a], u[a]);
+            }
+        }
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[a] = min(mn[a], __shfl_xor_sync(0xFFFFFFFFu, mn[a], o));
+            mx[a] = max(mx[a], __shfl_xor_sync(0xFFFFFFFFu, mx[a], o));
+        }
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(sb + a, mn[a]);
+            atomicMax(sb + 3 + a, mx[a]);
+        }
+}
+
+__device__ inline float half_area3(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Priority of each triangle.  The box of a piece of a flat patch with unit
+// normal n and area A has half area at least 2 A (|nx| + |ny| + |nz|), which
+// is |c.x| + |c.y| + |c.z| for the whole triangle, c = (b - a) x (c - a);
+// the box's half area above that is what splitting can remove.
+__global__ void split_priority_kernel(const float* v, const int32_t* idx, int64_t n, const unsigned* sb,
+                                      float* prio) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t* ti = idx + 3 * t;
+    const float3 a = vtx(v, ti[0]), b = vtx(v, ti[1]), c = vtx(v, ti[2]);
+    const float lo[3] = {fminf(a.x, fminf(b.x, c.x)), fminf(a.y, fminf(b.y, c.y)), fminf(a.z, fminf(b.z, c.z))};
+    const float hi[3] = {fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y)), fmaxf(a.z, fmaxf(b.z, c.z))};
+    const float ex = b.x - a.x, ey = b.y - a.y, ez = b.z - a.z;
+    const float fx = c.x - a.x, fy = c.y - a.y, fz = c.z - a.z;
+    const float ideal = fabsf(ey * fz - ez * fy) + fabsf(ez * fx - ex * fz) + fabsf(ex * fy - ey * fx);
+    const float waste = half_area3(lo, hi) - ideal;
+    const SplitGrid g = split_grid(sb);
+    int axis = 0;
+    float pos = 0.f;
+    const int level = split_plane(g, lo, hi, axis, pos);
+    prio[t] = (level < 0 || !(waste > 0.f)) ? 0.f : exp2f((float)level / 3.f) * cbrtf(waste);
+}
+
+// Pieces per triangle: 1 + its share of the `extra` budget, at most kMaxPieces.
+__global__ void split_count_kernel(const float* prio, int64_t n, const float* sum, double extra, int64_t* pieces) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double s = (double)*sum;
+    const double share = s > 0.0 ? floor(extra * (double)prio[t] / s) : 0.0;
+    pieces[t] = 1 + (int64_t)fmin(share, (double)(kMaxPieces - 1));
+}
+
+// The part of triangle (a, b, c) on one side of the plane x[axis] = p (upper
+// side when `upper`), bounded in double and rounded outwards, clipped to box
+// [blo, bhi].  Returns false when that part misses the box.
+__device__ bool clip_side(const double3 (&tri)[3], int axis, double p, bool upper, const float blo[3],
+                          const float bhi[3], float lo[3], float hi[3]) {
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    auto comp = [](const double3& q, int a) { return a == 0 ? q.x : (a == 1 ? q.y : q.z); };
+    auto add = [&](double x, double y, double z) {
+        mn[0] = fmin(mn[0], x); mx[0] = fmax(mx[0], x);
+        mn[1] = fmin(mn[1], y); mx[1] = fmax(mx[1], y);
+        mn[2] = fmin(mn[2], z); mx[2] = fmax(mx[2], z);
+    };
+    bool any = false;
+    for (int i = 0; i < 3; ++i) {
+        const double3& q = tri[i];
+        const double qi = comp(q, axis);
+        if (upper ? qi >= p : qi <= p) {
+            add(q.x, q.y, q.z);
+            any = true;
+        }
+        const double3& r = tri[(i + 1) % 3];
+        const double ri = comp(r, axis);
+        if ((qi < p && ri > p) || (qi > p && ri < p)) {
+            const double s = (p - qi) / (ri - qi);
+            double x = q.x + s * (r.x - q.x), y = q.y + s * (r.y - q.y), z = q.z + s * (r.z - q.z);
+            if (axis == 0) x = p; else if (axis == 1) y = p; else z = p;
+            add(x, y, z);
+            any = true;
+        }
+    }
+    if (!any) return false;
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = fmaxf(__double2float_rd(mn[a]), blo[a]);
+        hi[a] = fminf(__double2float_ru(mx[a]), bhi[a]);
+        if (!(lo[a] <= hi[a])) return false;
+    }
+    return true;
+}
+
+// Cuts triangle t into pieces[t] references at off[t]: the box mesh (two
+// corners per reference in rv, the triangle (2r, 2r + 1, 2r + 1) in ri) and
+// the triangle of each reference (rtri).  Pieces are taken depth-first, the
+// plane of each cut by split_plane, the pieces of a box shared between its
+// two sides by their half areas; a box no plane cuts is one reference and
+// any slots left over repeat the last reference.
+struct SplitEntry {
+    float lo[3], hi[3];
+    int count;
+};
+
+__global__ void split_kernel(const float* v, const int32_t* idx, int64_t n, const unsigned* sb,
+                             const int64_t* pieces, const int64_t* off, float* rv, int32_t* ri, int32_t* rtri) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t* ti = idx + 3 * t;
+    double3 tri[3];
+    float lo[3], hi[3];
+    for (int c = 0; c < 3; ++c) {
+        const float3 p = vtx(v, ti[c]);
+        tri[c] = make_double3(p.x, p.y, p.z);
+    }
+    for (int a = 0; a < 3; ++a) {
+        const float x0 = a == 0 ? (float)tri[0].x : (a == 1 ? (float)tri[0].y : (float)tri[0].z);
+        const float x1 = a == 0 ? (float)tri[1].x : (a == 1 ? (float)tri[1].y : (float)tri[1].z);
+        const float x2 = a == 0 ? (float)tri[2].x : (a == 1 ? (float)tri[2].y : (float)tri[2].z);
+        lo[a] = fminf(x0, fminf(x1, x2));
+        hi[a] = fmaxf(x0, fmaxf(x1, x2));
+    }
+    const int total = (int)(pieces[t] < kMaxPieces ? pieces[t] : kMaxPieces);
+    const int64_t base = off[t];
+    const SplitGrid g = split_grid(sb);
+    SplitEntry st[kMaxPieces];
+    int sp = 0, emitted = 0, steps = 0;
+    st[sp++] = SplitEntry{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}, total};
+    float last[6] = {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]};
+    auto emit = [&](const float* elo, const float* ehi) {
+        if (emitted >= total) return;
+        const int64_t r = base + emitted++;
+        for (int a = 0; a < 3; ++a) {
+            rv[6 * r + a] = elo[a];
+            rv[6 * r + 3 + a] = ehi[a];
+            last[a] = elo[a];
+            last[3 + a] = ehi[a];
+        }
+        ri[3 * r] = (int32_t)(2 * r);
+        ri[3 * r + 1] = (int32_t)(2 * r + 1);
+        ri[3 * r + 2] = (int32_t)(2 * r + 1);
+        rtri[r] = (int32_t)t;
+    };
+    while (sp > 0 && emitted < total) {
+        const SplitEntry e = st[--sp];
+        int axis = 0;
+        float pos = 0.f;
+        if (e.count == 1 || ++steps > 4 * kMaxPieces || split_plane(g, e.lo, e.hi, axis, pos) < 0) {
+            emit(e.lo, e.hi);
+            continue;
+        }
+        SplitEntry L, R;
+        const bool okl = clip_side(tri, axis, (double)pos, false, e.lo, e.hi, L.lo, L.hi);
+        const bool okr = clip_side(tri, axis, (double)pos, true, e.lo, e.hi, R.lo, R.hi);
+        if (!okl && !okr) {
+            emit(e.lo, e.hi);
+            continue;
+        }
+        if (!okl || !okr) {  // all pieces to the one side that holds the triangle
+            SplitEntry& o = okl ? L : R;
+            o.count = e.count;
+            st[sp++] = o;
+            continue;
+        }
+        const float al = half_area3(L.lo, L.hi), ar = half_area3(R.lo, R.hi);
+        int cl = (al + ar > 0.f) ? __float2int_rn((float)e.count * al / (al + ar)) : e.count / 2;
+        cl = max(1, min(e.count - 1, cl));
+        L.count = cl;
+        R.count = e.count - cl;
+        st[sp++] = R;  // counts on the stack never exceed total <= kMaxPieces entries
+        st[sp++] = L;
+    }
+    while (emitted < total) emit(last, last + 3);
 }
 
 // Centroid bounds as order-preserving unsigned min / max (6 words).
@@ -502,7 +744,7 @@ __global__ void collapse_dp_kernel(const uint64_t* k, uint64_t idx_mask, int64_t
 // the collapse chose them.
 __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, int64_t next_cap, const BNode* nodes,
                               const uint64_t* k, uint64_t idx_mask, const float* v, const int32_t* idx,
-                              float4* out_nodes,
+                              const float* tv, const int32_t* tidx, const int32_t* ref_tri, float4* out_nodes,
                               int64_t node_cap, float4* woop, int32_t* prim, int64_t tri_cap, Ctr* ctr,
                               const CollapseDP* dp) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -642,10 +884,11 @@ __global__ void expand_kernel(const Item* items, int64_t n_items, Item* next, in
                     return;
                 }
                 if (x < 0) {
-                    const int64_t tri = key_tri(k, ~x, idx_mask);
+                    const int64_t ref = key_tri(k, ~x, idx_mask);
+                    const int64_t tri = ref_tri ? (int64_t)ref_tri[ref] : ref;
                     const int64_t slot = (int64_t)tbase + leaf_tris;
-                    const int32_t* ti = idx + 3 * tri;
-                    woopify_dev(vtx(v, ti[0]), vtx(v, ti[1]), vtx(v, ti[2]), woop + 3 * slot);
+                    const int32_t* ti = tidx + 3 * tri;
+                    woopify_dev(vtx(tv, ti[0]), vtx(tv, ti[1]), vtx(tv, ti[2]), woop + 3 * slot);
                     prim[3 * slot] = (int32_t)tri;
                     prim[3 * slot + 1] = -1;
                     prim[3 * slot + 2] = -1;
@@ -872,12 +1115,113 @@ static rq_status ploc_tree(const uint64_t* keys_sorted, uint64_t idx_mask, int64
     return st;
 }
 
+// The references of a pre-split mesh: the box mesh (2 corners per
+// reference), its index triples and the triangle of each reference.
+struct RefMesh {
+    float* v = nullptr;
+    int32_t* idx = nullptr;
+    int32_t* tri = nullptr;
+    int64_t n = 0;
+    void release() {
+        cudaFree(v);
+        cudaFree(idx);
+        cudaFree(tri);
+        *this = RefMesh{};
+    }
+};
+
+// Cuts the nt triangles into at most nt + nt * budget / 100 references
+// (fewer when few triangles waste box area).  Leaves rm.n = 0 when there is
+// nothing to split.  The indices have been checked.
+static rq_status presplit(const float* v, const int32_t* idx, int64_t nt, int budget, RefMesh& rm, cudaStream_t s) {
+    const int64_t extra = std::min<int64_t>((int64_t)((double)nt * budget / 100.0), (int64_t)INT32_MAX / 4 - nt);
+    if (extra <= 0) return RQ_OK;
+    rq_status st = RQ_OK;
+    auto ok = [&](cudaError_t e) {
+        if (e != cudaSuccess && st == RQ_OK) st = cuda_fail(e, "rq_build_scene_gpu (split)");
+        return st == RQ_OK;
+    };
+    unsigned* sb = nullptr;
+    float *prio = nullptr, *sum = nullptr;
+    int64_t *pieces = nullptr, *off = nullptr;
+    void* temp = nullptr;
+    size_t b_sum = 0, b_scan = 0;
+    int64_t refs = 0;
+    if (ok(cudaMalloc(&sb, 6 * sizeof(unsigned))) && ok(cudaMalloc(&prio, nt * sizeof(float))) &&
+        ok(cudaMalloc(&sum, sizeof(float))) && ok(cudaMalloc(&pieces, nt * sizeof(int64_t))) &&
+        ok(cudaMalloc(&off, nt * sizeof(int64_t))) &&
+        ok(cub::DeviceReduce::Sum(nullptr, b_sum, prio, sum, (int)nt, s)) &&
+        ok(cub::DeviceScan::ExclusiveSum(nullptr, b_scan, pieces, off, (int)nt, s)) &&
+        ok(cudaMalloc(&temp, std::max<size_t>({b_sum, b_scan, (size_t)1})))) {
+        const unsigned init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+        ok(cudaMemcpyAsync(sb, init, sizeof(init), cudaMemcpyHostToDevice, s));
+        scene_bounds_kernel<<<std::min<unsigned>(blocks_of(nt, 256), 4 * 148), 256, 0, s>>>(v, idx, nt, sb);
+        split_priority_kernel<<<blocks_of(nt, 256), 256, 0, s>>>(v, idx, nt, sb, prio);
+        ok(cudaGetLastError());
+        ok(cub::DeviceReduce::Sum(temp, b_sum, prio, sum, (int)nt, s));
+        split_count_kernel<<<blocks_of(nt, 256), 256, 0, s>>>(prio, nt, sum, (double)extra, pieces);
+        ok(cudaGetLastError());
+        ok(cub::DeviceScan::ExclusiveSum(temp, b_scan, pieces, off, (int)nt, s));
+        int64_t tail[2] = {0, 0};
+        ok(cudaMemcpyAsync(&tail[0], off + nt - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        ok(cudaMemcpyAsync(&tail[1], pieces + nt - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        ok(cudaStreamSynchronize(s));
+        refs = tail[0] + tail[1];
+        if (st == RQ_OK && (refs < nt || refs > (int64_t)INT32_MAX / 4)) st = RQ_ERR_INVALID_ARG;
+    }
+    if (st == RQ_OK && refs > nt) {
+        if (ok(cudaMalloc(&rm.v, refs * 6 * sizeof(float))) && ok(cudaMalloc(&rm.idx, refs * 3 * sizeof(int32_t))) &&
+            ok(cudaMalloc(&rm.tri, refs * sizeof(int32_t)))) {
+            split_kernel<<<blocks_of(nt, 128), 128, 0, s>>>(v, idx, nt, sb, pieces, off, rm.v, rm.idx, rm.tri);
+            ok(cudaGetLastError());
+            rm.n = refs;
+        }
+    }
+    if (st != RQ_OK) rm.release();
+    ok(cudaStreamSynchronize(s));  // the temporaries below are freed after the kernels that read them
+    cudaFree(sb);
+    cudaFree(prio);
+    cudaFree(sum);
+    cudaFree(pieces);
+    cudaFree(off);
+    cudaFree(temp);
+    return st;
+}
+
 extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt,
-                                        int method, int optimize_passes, rq_scene_t* out, void* stream) {
+                                        int method, int optimize_passes, int split_budget, rq_scene_t* out,
+                                        void* stream) {
     if (!out || !vertices || !indices || nv <= 0 || nt <= 0 || nt > (int64_t)INT32_MAX / 4) return RQ_ERR_INVALID_ARG;
     if (method != RQ_GPU_BUILD_LBVH && method != RQ_GPU_BUILD_PLOC) return RQ_ERR_INVALID_ARG;
+    if (split_budget < 0 || split_budget > 400) return RQ_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
-    const int64_t n = nt;
+    {
+        // indices first: every kernel below reads vertices through them
+        unsigned* bad_d = nullptr;
+        unsigned bad = 0;
+        RQ_CUDA(cudaMalloc(&bad_d, sizeof(unsigned)));
+        cudaError_t e = cudaMemsetAsync(bad_d, 0, sizeof(unsigned), s);
+        if (e == cudaSuccess) {
+            check_indices_kernel<<<std::min<unsigned>(blocks_of(3 * nt, 256), 8 * 148), 256, 0, s>>>(
+                indices, 3 * nt, nv, bad_d);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, bad_d, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaFree(bad_d);
+        if (e != cudaSuccess) return cuda_fail(e, "rq_build_scene_gpu");
+        if (bad) return RQ_ERR_INVALID_ARG;
+    }
+    RefMesh rm;
+    if (split_budget > 0) {
+        const rq_status ps = presplit(vertices, indices, nt, split_budget, rm, s);
+        if (ps != RQ_OK) return ps;
+    }
+    // The tree stages read boxes from the box mesh when the triangles were
+    // split, from the triangles otherwise; leaves map back through rm.tri.
+    const float* bv = rm.n ? rm.v : vertices;
+    const int32_t* bi = rm.n ? rm.idx : indices;
+    const int64_t n = rm.n ? rm.n : nt;
     // device scratch
     uint64_t *keys = nullptr, *keys_sorted = nullptr;
     BNode* bn = nullptr;
@@ -924,19 +1268,8 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
         ok(cudaMemsetAsync(ctr, 0, sizeof(Ctr), s), "rq_build_scene_gpu");
     }
     if (st == RQ_OK) {
-        // indices first: the kernels below read vertices through them
-        unsigned bad = 0;
-        ok(cudaMemsetAsync(&ctr->error, 0, sizeof(unsigned), s), "rq_build_scene_gpu");
-        check_indices_kernel<<<std::min<unsigned>(blocks_of(3 * n, 256), 8 * 148), 256, 0, s>>>(indices, 3 * n, nv,
-                                                                                                 &ctr->error);
-        ok(cudaGetLastError(), "rq_build_scene_gpu");
-        ok(cudaMemcpyAsync(&bad, &ctr->error, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "rq_build_scene_gpu");
-        ok(cudaStreamSynchronize(s), "rq_build_scene_gpu");
-        if (st == RQ_OK && bad) st = RQ_ERR_INVALID_ARG;
-    }
-    if (st == RQ_OK) {
-        centroid_bounds_kernel<<<std::min<unsigned>(blocks_of(n, 256), 4 * 148), 256, 0, s>>>(vertices, indices, n, ob);
-        morton_kernel<<<blocks_of(n, 256), 256, 0, s>>>(vertices, indices, n, ob, axis_bits, idx_bits, keys);
+        centroid_bounds_kernel<<<std::min<unsigned>(blocks_of(n, 256), 4 * 148), 256, 0, s>>>(bv, bi, n, ob);
+        morton_kernel<<<blocks_of(n, 256), 256, 0, s>>>(bv, bi, n, ob, axis_bits, idx_bits, keys);
         ok(cudaGetLastError(), "rq_build_scene_gpu");
         ok(cub::DeviceRadixSort::SortKeys(nullptr, cub_bytes, keys, keys_sorted, (int)n, 0, end_bit, s),
            "rq_build_scene_gpu");
@@ -947,22 +1280,22 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
     int64_t levels = 0, n_nodes = 1;
     if (st == RQ_OK && n > 1) {
         if (method == RQ_GPU_BUILD_PLOC) {
-            st = ploc_tree(keys_sorted, idx_mask, n, vertices, indices, bn, leaf_parent, s);
+            st = ploc_tree(keys_sorted, idx_mask, n, bv, bi, bn, leaf_parent, s);
         } else {
             radix_tree_kernel<<<blocks_of(n - 1, 256), 256, 0, s>>>(keys_sorted, n, bn, leaf_parent);
-            boxes_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,
+            boxes_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, bv, bi, bn,
                                                            leaf_parent, arrivals);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
         }
         for (int pass = 0; pass < optimize_passes && st == RQ_OK; ++pass) {
             ok(cudaMemsetAsync(arrivals, 0, (n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
-            treelet_kernel<<<blocks_of(n, 128), 128, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,
+            treelet_kernel<<<blocks_of(n, 128), 128, 0, s>>>(keys_sorted, idx_mask, n, bv, bi, bn,
                                                              leaf_parent, arrivals, kTreeletLeaves);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
         }
         if (st == RQ_OK) {
             ok(cudaMemsetAsync(arrivals, 0, (n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
-            collapse_dp_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, vertices, indices, bn,
+            collapse_dp_kernel<<<blocks_of(n, 256), 256, 0, s>>>(keys_sorted, idx_mask, n, bv, bi, bn,
                                                                  leaf_parent, arrivals, dp);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
         }
@@ -976,7 +1309,8 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
         int64_t n_items = 1;
         while (st == RQ_OK && n_items > 0) {
             expand_kernel<<<blocks_of(n_items, 128), 128, 0, s>>>(qa, n_items, qb, q_cap, bn, keys_sorted, idx_mask,
-                                                                  vertices, indices, nodes, node_cap, woop, prim, n,
+                                                                  bv, bi, vertices, indices, rm.tri, nodes, node_cap,
+                                                                  woop, prim, n,
                                                                   ctr, n > 1 ? dp : nullptr);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
             Ctr c{};
@@ -1007,6 +1341,7 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
     cudaFree(qb);
     cudaFree(ctr);
     cudaFree(cub_temp);
+    rm.release();
     if (st != RQ_OK) {
         cudaFree(nodes);
         cudaFree(woop);

@@ -489,20 +489,25 @@ rq_status rq_device_free(void* p);
  * floats) and indices (3*nt ints) on `stream`.  The binary tree comes from
  * the triangles in Morton order, either as Karras's radix tree
  * (RQ_GPU_BUILD_LBVH: fastest) or by parallel locally-ordered clustering
- * (RQ_GPU_BUILD_PLOC: merged boxes of least area; better trees), then
+ * (RQ_GPU_BUILD_PLOC: merged boxes of least area; better trees).  With
+ * `split_budget` > 0 (percent of nt, at most 400; 0 = none) triangles whose
+ * boxes are much larger than they are are first cut into references along
+ * a grid's planes (Karras and Aila 2013), at most nt * split_budget / 100
+ * extra, and a triangle may then be stored more than once.  Then
  * `optimize_passes` bottom-up passes of treelet restructuring (7-leaf
  * treelets rebuilt SAH-optimally; 0 = none), then a top-down collapse to
  * 8-wide nodes written in the CWBVH format with Woop rows and the primitive
  * map.  Much faster to build than rq_build_bvh, slower to trace; the scene
  * owns its buffers (rq_scene_destroy).  No reference counterpart (the
  * reference builds on the host with Embree).  Indices outside [0, nv) give
- * RQ_ERR_INVALID_ARG.  Synchronises `stream` once per tree level (and once
- * per clustering round).
+ * RQ_ERR_INVALID_ARG, as do an unknown method and a budget outside
+ * [0, 400].  Synchronises `stream` once per tree level (and once per
+ * clustering round).
  */
 #define RQ_GPU_BUILD_LBVH 0
 #define RQ_GPU_BUILD_PLOC 1
 rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt, int method,
-                             int optimize_passes, rq_scene_t* out, void* stream);
+                             int optimize_passes, int split_budget, rq_scene_t* out, void* stream);
 
 /* ------------------------------------------------------- instancing (TLAS) */
 /*

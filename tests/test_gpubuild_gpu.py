@@ -1,8 +1,9 @@
 """CWBVH scenes built on the GPU (rq_build_scene_gpu): a valid CWBVH that the
 trace kernels and the oracle traverse identically, every triangle stored
-once with the host Woop transform's rows, and the same answers as the host
-SAH build of the same mesh (occlusion identical, closest triangles
-identical up to ties, disagreements explained in FP64)."""
+with the host Woop transform's rows (once, or within the split budget when
+triangles are pre-split), and the same answers as the host SAH build of the
+same mesh (occlusion identical, closest triangles identical up to ties,
+disagreements explained in FP64)."""
 import numpy as np
 import pytest
 
@@ -17,38 +18,44 @@ def _device_mesh(V, I):
         torch.from_numpy(np.ascontiguousarray(I, np.int32)).cuda()
 
 
-@pytest.fixture(scope="module", params=[(0, 0), (0, 2), (1, 0), (1, 2)],
-                ids=["lbvh", "lbvh-treelets", "ploc", "ploc-treelets"])
+@pytest.fixture(scope="module", params=[(0, 0, 0), (0, 2, 0), (1, 0, 0), (1, 2, 0), (0, 0, 100), (1, 2, 30)],
+                ids=["lbvh", "lbvh-treelets", "ploc", "ploc-treelets", "lbvh-split100", "ploc-treelets-split30"])
 def built(rq, request):
     from cwbvh_b200 import workloads as W
     V, I = W.scene_of_size(3, 150_000)
     v, i = _device_mesh(V, I)
-    method, passes = request.param
-    sc = rq.Scene.build_gpu(v, i, optimize_passes=passes, method=method)
+    method, passes, budget = request.param
+    sc = rq.Scene.build_gpu(v, i, optimize_passes=passes, method=method, split_budget=budget)
     nodes, woop, prim = sc.download()
-    return V, I, v, i, sc, nodes, woop, prim
+    return V, I, v, i, sc, nodes, woop, prim, budget
 
 
 def test_layout_and_woop_rows(rq, built):
-    V, I, v, i, sc, nodes, woop, prim = built
+    V, I, v, i, sc, nodes, woop, prim, budget = built
     n = I.shape[0]
-    assert woop.shape == (3 * n, 4) and prim.shape == (3 * n,)
     ids = prim.reshape(-1, 3)
+    refs = ids.shape[0]
+    assert woop.shape == (3 * refs, 4) and prim.shape == (3 * refs,)
     assert (ids[:, 1:] == -1).all()
-    assert np.array_equal(np.sort(ids[:, 0]), np.arange(n))  # every triangle once
+    if budget == 0:
+        assert np.array_equal(np.sort(ids[:, 0]), np.arange(n))  # every triangle once
+    else:
+        # every triangle at least once, the extra references within the budget
+        assert np.array_equal(np.unique(ids[:, 0]), np.arange(n))
+        assert n < refs <= n + n * budget // 100 + 64
     rows = woop.reshape(-1, 3, 4)
-    for slot in np.random.default_rng(0).integers(0, n, 300):
+    for slot in np.random.default_rng(0).integers(0, refs, 300):
         t = I[ids[slot, 0]]
         want = rq.woopify(V[t[0]], V[t[1]], V[t[2]])
         assert np.array_equal(rows[slot].view(np.uint32), want.view(np.uint32))
-    assert 0 < nodes.shape[0] // 5 <= n
+    assert 0 < nodes.shape[0] // 5 <= refs
 
 
 @pytest.mark.parametrize("query", [0, 1], ids=["closest", "any"])
 def test_kernels_and_oracle_agree_on_gpu_tree(rq, po, built, query):
     import torch
     from cwbvh_b200 import workloads as W
-    V, I, v, i, sc, nodes, woop, prim = built
+    V, I, v, i, sc, nodes, woop, prim, _ = built
     hb = rq.HostBVH(V, I, rq.CWBVH)
     ref = W.DeviceScene(rq.CWBVH, hb, rq.Scene.from_host(hb), v, i, W.diag(V), I.shape[0])
     rays = W.ao_rays(ref, 200_000, seed=17)
@@ -78,7 +85,7 @@ def test_small_and_invalid_meshes(rq, po):
              for method in (rq.GPU_BUILD_LBVH, rq.GPU_BUILD_PLOC)]
     for I, method in cases:
         v, i = _device_mesh(V, I)
-        sc = rq.Scene.build_gpu(v, i, method=method)
+        sc = rq.Scene.build_gpu(v, i, method=method, split_budget=400)
         nodes, woop, prim = sc.download()
         rays = np.zeros((64, 8), np.float32)
         rays[:, 0:3] = [0.2, 0.2, -1.0]
@@ -98,6 +105,9 @@ def test_small_and_invalid_meshes(rq, po):
     v, i = _device_mesh(V, np.array([[0, 1, 2]], np.int32))
     with pytest.raises(rq.RQError, match="INVALID_ARG"):
         rq.Scene.build_gpu(v, i, method=7)
+    for budget in (-1, 401):
+        with pytest.raises(rq.RQError, match="INVALID_ARG"):
+            rq.Scene.build_gpu(v, i, split_budget=budget)
 
 
 def test_duplicated_geometry(rq, po):
