@@ -402,6 +402,10 @@ rq_status rq_autotune_batch(rq_ctx_t ctx, const rq_batch_item* items, int n_item
                 }
             }
     if (st == RQ_OK) {
+        // The first stage ran with the default refill thresholds and ratio:
+        // write them out, so that a first-stage winner the second stage does
+        // not beat is returned (and cached) as the explicit launch it ran.
+        best.launch = resolve_launch(items[0].scene->kind, query, &best.launch);
         const rq_batch_params shape = best;
         const bool cw = items[0].scene->kind == RQ_BVH_CWBVH;
         for (const FetchChoice& fc : kFetchChoices)
