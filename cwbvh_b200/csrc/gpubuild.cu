@@ -514,21 +514,27 @@ __device__ void restructure(BNode* nodes, const uint64_t* k, uint64_t idx_mask, 
     }
     if (n_leaf < 3) return;
     const int full = (1 << n_leaf) - 1;
-    float cost[1 << kTreeletLeaves], blo[1 << kTreeletLeaves][3], bhi[1 << kTreeletLeaves][3];
+    // Subset boxes are recomputed from the leaves when needed instead of
+    // kept per subset: min / max are exact in any order, so the boxes are
+    // the same, and the per-thread table shrinks from 3.7 KB to 640 B.
+    auto subset_box = [&](int S, float lo[3], float hi[3]) {
+        for (int a = 0; a < 3; ++a) { lo[a] = FLT_MAX; hi[a] = -FLT_MAX; }
+        for (int q = 0; q < n_leaf; ++q)
+            if (S & (1 << q))
+                for (int a = 0; a < 3; ++a) { lo[a] = fminf(lo[a], llo[q][a]); hi[a] = fmaxf(hi[a], lhi[q][a]); }
+    };
+    float cost[1 << kTreeletLeaves];
     uint8_t part[1 << kTreeletLeaves];
     for (int S = 1; S <= full; ++S) {
         const int low = __ffs(S) - 1;
         const int rest = S & (S - 1);
         if (rest == 0) {
-            for (int a = 0; a < 3; ++a) { blo[S][a] = llo[low][a]; bhi[S][a] = lhi[low][a]; }
             cost[S] = lcost[low];
             part[S] = 0;
             continue;
         }
-        for (int a = 0; a < 3; ++a) {
-            blo[S][a] = fminf(blo[rest][a], llo[low][a]);
-            bhi[S][a] = fmaxf(bhi[rest][a], lhi[low][a]);
-        }
+        float slo[3], shi[3];
+        subset_box(S, slo, shi);
         float best = FLT_MAX;
         int bp = 0;
         // partitions {P, S \ P} with the lowest leaf in P, P != S
@@ -537,7 +543,7 @@ __device__ void restructure(BNode* nodes, const uint64_t* k, uint64_t idx_mask, 
             const float c = cost[P] + cost[S ^ P];
             if (c < best) { best = c; bp = P; }
         }
-        cost[S] = kCt * half_area(blo[S], bhi[S]) + best;
+        cost[S] = kCt * half_area(slo, shi) + best;
         part[S] = (uint8_t)bp;
     }
     if (!(cost[full] < 0.999f * __ldcg(&nodes[root].cost))) return;
@@ -584,7 +590,9 @@ __device__ void restructure(BNode* nodes, const uint64_t* k, uint64_t idx_mask, 
         BNode& b = nodes[nd];
         b.left = code[0];
         b.right = code[1];
-        for (int a = 0; a < 3; ++a) { b.lo[a] = blo[S][a]; b.hi[a] = bhi[S][a]; }
+        float slo[3], shi[3];
+        subset_box(S, slo, shi);
+        for (int a = 0; a < 3; ++a) { b.lo[a] = slo[a]; b.hi[a] = shi[a]; }
         int32_t cnt = 0;
         for (int q = 0; q < n_leaf; ++q)
             if (S & (1 << q)) cnt += lcnt[q];
