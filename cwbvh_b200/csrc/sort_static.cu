@@ -2,17 +2,18 @@
 // device allocation.
 //
 // Some callers cannot call cudaMalloc: a plugin running inside a host
-// application that owns all device memory through its own pool, code that
-// runs while the host is capturing its stream into a CUDA graph, or a service
-// whose memory budget was fixed when it started.  rq_sort_rays creates its
-// sort buffers on every call, so such callers use this entry point instead.
-// Its scratch (keys, values, the one-item table and the radix-sort temp
-// storage) lives in one file-scope device array of kScratchBytes, which every
-// GPU that loads librq holds until the process exits; that bounds a call to
-// RQ_SORT_STATIC_MAX_RAYS rays.
+// application that owns all device memory through its own pool, or a service
+// whose device-memory budget was fixed when it started.  rq_sort_rays creates
+// its sort buffers on every call, so such callers use this entry point
+// instead.  Its scratch (keys, values, the one-item table and the radix-sort
+// temp storage) lives in one file-scope device array of kScratchBytes, which
+// every GPU that loads librq holds until the process exits; that bounds a
+// call to RQ_SORT_STATIC_MAX_RAYS rays.
 //
 // The pipeline is rq_sort_rays's own: the same key and gather kernels and the
-// same radix sort, so the outputs are identical.
+// same radix sort, so the outputs are identical.  The one-item table and the
+// bounds are written into the array by a one-thread kernel that receives them
+// as launch arguments, so no host memory is read after the call returns.
 //
 // Set-up: the first call on each device (with that device current) looks up
 // the array's device address with cudaGetSymbolAddress and sizes the sort's
@@ -20,6 +21,7 @@
 // shares the array and leaves its contents behind; each call writes every
 // scratch byte it reads, so nothing needs clearing.  Calls whose work
 // overlaps on the GPU (other streams, other host threads) race on the array.
+// The call is stream-ordered: it returns with its work queued on `stream`.
 #include <cub/device/device_radix_sort.cuh>
 
 #include <mutex>
@@ -36,6 +38,15 @@ __global__ void gather_rays_kernel(const TraceItem* __restrict__ items, const ui
                                    const int32_t* __restrict__ vals, int64_t total, Ray* __restrict__ sorted);
 
 namespace {
+
+// Writes the one-item table and the bounds into the static scratch.
+__global__ void static_sort_setup_kernel(TraceItem item, float3 lo, float3 hi, TraceItem* items, float* bounds) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        items[0] = item;
+        bounds[0] = lo.x; bounds[1] = lo.y; bounds[2] = lo.z;
+        bounds[3] = hi.x; bounds[4] = hi.y; bounds[5] = hi.z;
+    }
+}
 
 constexpr int64_t kMaxRays = RQ_SORT_STATIC_MAX_RAYS;
 constexpr size_t kScratchBytes = 20u << 20;  // 20 MiB: 10 MiB of keys/values + the sort's ~6.1 MiB temp
@@ -125,17 +136,16 @@ extern "C" rq_status rq_sort_rays_static(const rq_ray* rays, int64_t count, cons
     item.rays = reinterpret_cast<const Ray*>(rays);
     item.ray_begin = 0;
     item.count = count;
-    const float bounds[6] = {bounds_lo[0], bounds_lo[1], bounds_lo[2], bounds_hi[0], bounds_hi[1], bounds_hi[2]};
-    // Pageable sources: these copies complete their read of the host values
-    // before returning.
-    RQ_CUDA(cudaMemcpyAsync(b + kItemOff, &item, sizeof(item), cudaMemcpyHostToDevice, strm));
-    RQ_CUDA(cudaMemcpyAsync(b + kBoundsOff, bounds, sizeof(bounds), cudaMemcpyHostToDevice, strm));
-    auto* items = reinterpret_cast<const TraceItem*>(b + kItemOff);
+    auto* items = reinterpret_cast<TraceItem*>(b + kItemOff);
+    auto* bounds = reinterpret_cast<float*>(b + kBoundsOff);
+    static_sort_setup_kernel<<<1, 32, 0, strm>>>(item, make_float3(bounds_lo[0], bounds_lo[1], bounds_lo[2]),
+                                                  make_float3(bounds_hi[0], bounds_hi[1], bounds_hi[2]), items,
+                                                  bounds);
+    RQ_CUDA(cudaGetLastError());
     auto* keys_in = reinterpret_cast<uint64_t*>(b + kKeysInOff);
     auto* keys_out = reinterpret_cast<uint64_t*>(b + kKeysOutOff);
     auto* vals_in = reinterpret_cast<int32_t*>(b + kValsInOff);
-    morton_keys_kernel<<<blocks_for(count, 256), 256, 0, strm>>>(items, 1, reinterpret_cast<const float*>(b + kBoundsOff),
-                                                                 count, keys_in, vals_in);
+    morton_keys_kernel<<<blocks_for(count, 256), 256, 0, strm>>>(items, 1, bounds, count, keys_in, vals_in);
     RQ_CUDA(cudaGetLastError());
     size_t tb = s->temp_bytes;
     RQ_CUDA(cub::DeviceRadixSort::SortPairs(b + kTempOff, tb, keys_in, keys_out, vals_in, perm, count, 0, kEndBit,

@@ -215,6 +215,31 @@ rq_status rq_trace_ao(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, int64_
 rq_status rq_trace_ordered(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,
                            int64_t count, rq_query query, void* stream);
 
+/* ------------------------------------------------- several GPUs, one ray set */
+/*
+ * One ray buffer traced over several devices holding replicas of one scene:
+ * the multi-GPU form of rtTraceCWBVH / rtTraceBVH2
+ * (src/TraversalKernelCWBVH.cu:387-426, src/TraversalKernelBVH2.cu:190-227).
+ * Rays [0, count) split into n_parts contiguous ranges (rq_shard_range: sizes
+ * differ by at most one, larger ranges first); range k is traced on
+ * devices[k] against scenes[k] (a replica created on that device).  The
+ * caller's rays and hits live on devices[0]: range 0 is traced there in
+ * place, every other device copies its range in (peer copy into its own
+ * staging buffer), traces it and copies its hits back into `hits`.  Devices
+ * may repeat.  The trace waits for `stream` (devices[0]) before it starts and
+ * returns when every hit is in place, with the first error any part met
+ * (kernel errors included, as rq_ctx_check reports them).
+ */
+typedef struct rq_sharded* rq_sharded_t;
+rq_status rq_shard_range(int64_t count, int n_parts, int part, int64_t* begin, int64_t* size);
+/* Per part: a context, a stream and (parts 1..) staging buffers for
+ * ceil(max_rays / n_parts) rays on that part's device. */
+rq_status rq_sharded_create(int n_parts, const int* devices, const rq_scene_t* scenes, int64_t max_rays,
+                            rq_sharded_t* out);
+rq_status rq_sharded_trace(rq_sharded_t shards, const rq_ray* rays, rq_hit* hits, int64_t count,
+                           rq_query query, const rq_launch* launch, void* stream);
+rq_status rq_sharded_destroy(rq_sharded_t shards);
+
 /* Defaults used when rq_launch fields are zero (a negative postpone_ratio
  * turns triangle postponing off). */
 rq_status rq_default_launch(rq_bvh_kind kind, rq_query query, rq_launch* out);
@@ -280,16 +305,19 @@ rq_status rq_sort_rays(rq_ctx_t ctx, const rq_ray* rays, int64_t count, const fl
 
 /* rq_sort_rays without allocating device memory.  No counterpart in the
  * reference.  Some callers cannot call cudaMalloc -- a plugin inside a host
- * that owns all device memory through its own pool, code running while its
- * host captures the stream into a CUDA graph, a service whose memory budget
- * was fixed at start-up -- and rq_sort_rays allocates its sort buffers on
- * every call.  This entry point keeps its scratch in one static 20 MiB device
- * array that every GPU loading librq holds until exit, which limits a call to
- * RQ_SORT_STATIC_MAX_RAYS rays (larger counts return RQ_ERR_INVALID_ARG with
- * the limit in rq_last_error).  Outputs are identical to rq_sort_rays's.
- * The first call on a device (with that device current) looks up the array's
- * address; make it before any stream capture.  All calls share the array and
- * leave their contents in it: calls whose work overlaps on the GPU race. */
+ * that owns all device memory through its own pool, a service whose
+ * device-memory budget was fixed at start-up -- and rq_sort_rays allocates
+ * its sort buffers on every call.  This entry point keeps its scratch in one
+ * static 20 MiB device array that every GPU loading librq holds until exit,
+ * which limits a call to RQ_SORT_STATIC_MAX_RAYS rays (larger counts return
+ * RQ_ERR_INVALID_ARG with the limit in rq_last_error).  Outputs are identical
+ * to rq_sort_rays's.  Unlike rq_sort_rays, which waits for its stream, the
+ * call is stream-ordered and returns with its work queued on `stream`: keep
+ * `rays`, `sorted_rays` and `perm` alive until the stream has reached that
+ * point.  The first call on a device (with that device current) looks up the
+ * array's address; make it before any stream capture.  All calls share the
+ * array and leave their contents in it: calls whose work overlaps on the GPU
+ * race. */
 #define RQ_SORT_STATIC_MAX_RAYS 524288
 rq_status rq_sort_rays_static(const rq_ray* rays, int64_t count, const float bounds_lo[3],
                               const float bounds_hi[3], rq_ray* sorted_rays, int32_t* perm,
@@ -352,16 +380,22 @@ rq_status rq_autotune_batch(rq_ctx_t ctx, const rq_batch_item* items, int n_item
 
 /* ----------------------------------------------------------------- serving */
 /*
- * A continuous-batching AO bake server.  Requests (scene, host rays) are
- * admitted while their ray/hit buffers fit the HBM budget, gathered into
- * persistent batch launches on several streams (so batches overlap on the
- * device), and completed by copying hits back to the caller's host buffer.
+ * A continuous-batching AO bake server.  The HBM budget is one device pool
+ * allocated at creation; every request buffer lives in it.  Requests are cut
+ * into pieces of at most max_batch_rays rays (whole surfels for bake
+ * requests) that each fit the pool, so a request larger than one launch is
+ * split rather than refused.  Pieces are admitted in arrival order while the
+ * pool can give them their buffers (admission by bytes: the bytes in use
+ * never exceed the budget, and queued pieces wait for running ones to give
+ * theirs back), gathered into persistent batch launches on several streams
+ * (so batches overlap on the device), and completed by copying results back
+ * to the caller's host buffer; a request completes with its last piece.
  */
 typedef struct rq_server* rq_server_t;
 
 typedef struct rq_server_params {
-    int64_t hbm_budget_bytes;   /* ray+hit bytes admitted at once (48 B per ray) */
-    int64_t max_batch_rays;     /* cap on rays gathered into one launch          */
+    int64_t hbm_budget_bytes;   /* device pool for request buffers (48 B per ray of a ray request) */
+    int64_t max_batch_rays;     /* rays per launch and per piece (0 = budget / (48 x streams))      */
     int streams;                /* concurrent batch streams (default 3)          */
     rq_query query;
     rq_launch launch;
@@ -369,12 +403,22 @@ typedef struct rq_server_params {
 
 typedef struct rq_request_stats {
     double submit_ms;     /* host monotonic clock, ms                           */
-    double start_ms;      /* when its batch was launched                        */
-    double done_ms;       /* when its hits were back in the caller's buffer     */
+    double start_ms;      /* when its first piece was launched                  */
+    double done_ms;       /* when its last results were back in the caller's buffer */
     int64_t rays;
-    int32_t batch_id;
+    int32_t batch_id;     /* launch of its first piece                          */
     int32_t status;       /* rq_status of the request                           */
 } rq_request_stats;
+
+/* Pool accounting of a server (no reference counterpart). */
+typedef struct rq_server_memory_stats {
+    int64_t pool_bytes;         /* the HBM budget (rounded down to 256 B)           */
+    int64_t in_use_bytes;       /* held by admitted pieces now                      */
+    int64_t peak_in_use_bytes;  /* most ever held at once (<= pool_bytes)           */
+    int64_t admission_waits;    /* times the oldest queued piece waited for bytes   */
+    int64_t pieces;             /* pieces queued so far                             */
+    int64_t max_batch_rays;     /* rays per launch and per piece in effect          */
+} rq_server_memory_stats;
 
 rq_status rq_server_create(const rq_server_params* params, rq_server_t* out);
 rq_status rq_server_add_scene(rq_server_t server, rq_scene_t scene, int32_t* scene_id);
@@ -389,16 +433,20 @@ rq_status rq_server_submit(rq_server_t server, int32_t scene_id, const rq_ray* h
  * with the occluded rays counted per surfel in the trace epilogue; host_ao
  * (n_surfels floats) receives occluded / spp, equal to rq_aorays + rq_trace
  * + rq_ao_reduce.  Only the surfels (36 B each) go to the device and 4 B per
- * surfel come back.  The request occupies 36 B per surfel + 4 B per surfel +
- * 32 B per ray of arena (rounded to 256 B per buffer); RQ_ERR_BUDGET if that
- * exceeds one worker's arena, RQ_ERR_INVALID_ARG on a closest-hit server. */
+ * surfel come back.  A piece occupies 36 B per surfel + 4 B per surfel +
+ * 32 B per ray of the pool (rounded to 256 B per buffer); RQ_ERR_BUDGET if
+ * one surfel's rays exceed max_batch_rays or its buffers the pool,
+ * RQ_ERR_INVALID_ARG on a closest-hit server. */
 rq_status rq_server_submit_bake(rq_server_t server, int32_t scene_id, const float* host_pos,
                                 const float* host_nrm, const float* host_radius, int64_t n_surfels,
                                 int spp, uint64_t seed, float tmin, float tmax, float offset_scale,
                                 float* host_ao, uint64_t* ticket);
 rq_status rq_server_wait(rq_server_t server, uint64_t ticket, int64_t timeout_ms,
                          rq_request_stats* stats);
+/* Cancels a request none of whose pieces has started (RQ_ERR_NOT_FOUND
+ * otherwise); its wait returns RQ_ERR_CANCELLED. */
 rq_status rq_server_cancel(rq_server_t server, uint64_t ticket);
+rq_status rq_server_memory(rq_server_t server, rq_server_memory_stats* out);
 rq_status rq_server_destroy(rq_server_t server);
 
 /* ------------------------------------------------- procedural test scenes */
@@ -495,7 +543,8 @@ rq_status rq_device_free(void* p);
  * a grid's planes (Karras and Aila 2013), at most nt * split_budget / 100
  * extra, and a triangle may then be stored more than once.  Then
  * `optimize_passes` bottom-up passes of treelet restructuring (7-leaf
- * treelets rebuilt SAH-optimally; 0 = none), then a top-down collapse to
+ * treelets rebuilt SAH-optimally, a warp per treelet; 0 = none), then a
+ * top-down collapse to
  * 8-wide nodes written in the CWBVH format with Woop rows and the primitive
  * map.  Much faster to build than rq_build_bvh, slower to trace; the scene
  * owns its buffers (rq_scene_destroy).  No reference counterpart (the
@@ -506,6 +555,9 @@ rq_status rq_device_free(void* p);
  */
 #define RQ_GPU_BUILD_LBVH 0
 #define RQ_GPU_BUILD_PLOC 1
+/* OR-ed into `method`: restructure each treelet with one thread instead of
+ * one warp (slower; the same trees, byte for byte). */
+#define RQ_GPU_BUILD_THREAD_TREELETS 0x100
 rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const int32_t* indices, int64_t nt, int method,
                              int optimize_passes, int split_budget, rq_scene_t* out, void* stream);
 
@@ -548,13 +600,18 @@ rq_status rq_trace_instanced(rq_ctx_t ctx, rq_tlas_t tlas, const rq_ray* rays, r
 /* ------------------------------------------------------------- device info */
 int rq_device_sm_count(void);
 /* L2 read-bandwidth probe (a measurement utility; no reference counterpart):
- * every thread of a persistent grid (SMs x 8 blocks x 256 threads) reads
- * `buf` (device, `bytes` a multiple of 64, 16-byte aligned) `reps` times with
- * L1-bypassing 16-byte loads, and folds the words into `sink` (device,
+ * every thread of a grid of SMs x 8 blocks x 256 threads reads `buf`
+ * (device, `bytes` a multiple of 16, 16-byte aligned) `reps` times with
+ * coalesced L1-bypassing 16-byte loads (a warp's load covers 512 contiguous
+ * bytes), four in flight per thread, and folds the words into `sink` (device,
  * 4 bytes) only if they XOR to a magic value, so the loads stay live.  A
  * buffer well inside L2 gives the L2 read bandwidth: time the call with
  * events on `stream` and divide bytes * reps by the time. */
 rq_status rq_probe_l2_read(const void* buf, int64_t bytes, int reps, uint32_t* sink, void* stream);
+/* The same probe with its launch shape given: SMs x blocks_per_sm blocks
+ * (1..64) and `loads` (4 or 8) loads in flight per thread. */
+rq_status rq_probe_l2_read_shape(const void* buf, int64_t bytes, int reps, int blocks_per_sm, int loads,
+                                 uint32_t* sink, void* stream);
 /* Library build identification: "rq <version> sm_100a". */
 const char* rq_version(void);
 

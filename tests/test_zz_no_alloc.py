@@ -1,16 +1,16 @@
 """rq_sort_rays_static -- the Morton ray sort for callers that cannot call
-cudaMalloc (a plugin whose host owns all device memory, code running while
-its host captures the stream into a CUDA graph, a service with a memory
-budget fixed at start-up).  It keeps its scratch in a static device array
-instead of allocating.  Through the C ABI, two calls in a row must give the
-same sorted rays and permutation as rq_sort_rays, the allocating entry point,
-and a count above the array's limit must be refused with a clear error.
+cudaMalloc (a plugin whose host owns all device memory through its own pool,
+a service whose device-memory budget was fixed at start-up).  It keeps its
+scratch in a static device array instead of allocating.  Through the C ABI,
+two calls in a row must give the same sorted rays and permutation as
+rq_sort_rays, the allocating entry point; once the first calls have run,
+further calls must leave the device's free memory unchanged; and a count
+above the array's limit must be refused with a clear error.
 
 This file is collected last so that a failure here stops a run only after
 every other test has run."""
 import ctypes as C
 
-import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -18,11 +18,12 @@ pytestmark = pytest.mark.gpu
 MAX_RAYS = 524288  # RQ_SORT_STATIC_MAX_RAYS in include/rq.h
 
 
-def _static_sort(rq, rays, lo, hi):
+def _static_sort(rq, rays, lo, hi, out=None, perm=None):
     import torch
     n = rays.shape[0]
-    out = torch.empty_like(rays)
-    perm = torch.full((n,), -1, dtype=torch.int32, device=rays.device)
+    if out is None:
+        out = torch.empty_like(rays)
+        perm = torch.full((n,), -1, dtype=torch.int32, device=rays.device)
     st = rq.lib.rq_sort_rays_static(rays.data_ptr(), n, (C.c_float * 3)(*lo), (C.c_float * 3)(*hi),
                                     out.data_ptr(), perm.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert st == 0, rq.lib.rq_last_error()
@@ -30,12 +31,17 @@ def _static_sort(rq, rays, lo, hi):
     return out, perm
 
 
-def test_static_sort_matches_allocating_sort_twice(rq):
-    import torch
+def _scene(rq):
     from cwbvh_b200 import workloads as W
     V, I = W.heightfield_boxes(0)
     ds = W.upload(V, I, rq.CWBVH)
-    lo, hi = ds.host.info["bounds_lo"], ds.host.info["bounds_hi"]
+    return ds, ds.host.info["bounds_lo"], ds.host.info["bounds_hi"]
+
+
+def test_static_sort_matches_allocating_sort_twice(rq):
+    import torch
+    from cwbvh_b200 import workloads as W
+    ds, lo, hi = _scene(rq)
     ctx = rq.Context()
     # Two calls in a row on different ray sets: the second must not see the
     # first one's leftovers in the shared scratch.
@@ -47,6 +53,29 @@ def test_static_sort_matches_allocating_sort_twice(rq):
         assert torch.equal(got_perm, want_perm)
         assert torch.equal(got_rays, want_rays)
         assert torch.equal(got_rays, rays[got_perm.long()])
+
+
+def test_static_sort_allocates_nothing(rq):
+    import torch
+    from cwbvh_b200 import workloads as W
+    ds, lo, hi = _scene(rq)
+    cases = []
+    for n, seed in ((MAX_RAYS, 3000), (77_777, 4000)):
+        rays = W.ao_rays(ds, n, seed=seed)
+        cases.append((rays, torch.empty_like(rays), torch.empty((n,), dtype=torch.int32, device="cuda")))
+    # The first calls set up the device and load the kernels they launch.
+    for rays, out, perm in cases:
+        _static_sort(rq, rays, lo, hi, out, perm)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        for rays, out, perm in cases:
+            _static_sort(rq, rays, lo, hi, out, perm)
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    rays, out, perm = cases[1]
+    assert torch.equal(out, rays[perm.long()])
 
 
 def test_static_sort_refuses_more_than_its_limit(rq):
