@@ -170,22 +170,31 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def measure_l2_read(stream, mbytes: int = 48, reps: int = 100) -> float:
+def measure_l2_read(stream) -> dict:
     """L2 read bandwidth (GB/s) from the library's probe kernel
-    (rq_probe_l2_read): a 48 MB buffer, well inside the 126 MB L2, read
-    `reps` times with L1-bypassing 16-byte loads."""
+    (rq_probe_l2_read_shape): coalesced L1-bypassing 16-byte loads over an
+    L2-resident buffer, swept over buffer size (8/16/32/48 MB), grid
+    (SMs x 8/16/32 blocks of 256 threads) and loads in flight per thread
+    (4/8); the best shape is the peak."""
     import torch
     import cwbvh_b200 as rq
-    n = mbytes << 20
     with torch.cuda.stream(stream):
-        buf = torch.ones(n // 4, dtype=torch.int32, device="cuda")
+        buf = torch.ones((48 << 20) // 4, dtype=torch.int32, device="cuda")
         sink = torch.zeros(1, dtype=torch.int32, device="cuda")
-
-    def run():
-        rq.check(rq.lib.rq_probe_l2_read(buf.data_ptr(), n, reps, sink.data_ptr(), stream.cuda_stream),
-                 "rq_probe_l2_read")
-    ms = time_steps(run, 5, 3, stream)
-    return n * reps / (ms * 1e-3) / 1e9
+    sweep = []
+    for mb in (8, 16, 32, 48):
+        n = mb << 20
+        reps = max(1, (4 << 30) // n)  # ~4 GiB read per call
+        for bps in (8, 16, 32):
+            for loads in (4, 8):
+                def run():
+                    rq.check(rq.lib.rq_probe_l2_read_shape(buf.data_ptr(), n, reps, bps, loads, sink.data_ptr(),
+                                                           stream.cuda_stream), "rq_probe_l2_read_shape")
+                ms = time_steps(run, 5, 2, stream)
+                sweep.append({"mbytes": mb, "blocks_per_sm": bps, "loads": loads,
+                              "gbs": round(n * reps / (ms * 1e-3) / 1e9, 1)})
+    best = max(sweep, key=lambda r: r["gbs"])
+    return {"peak": best["gbs"], "best": best, "sweep": sweep}
 
 
 def measure_link(mbytes: int = 1024) -> dict:
@@ -293,6 +302,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving configuration")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="batched: skip the small, city and large configurations (run in their own processes)")
     ap.add_argument("--profile", action="store_true",
                     help="batched/small/large: build the workload and only run the trace W+K times (profiler captures)")
     args = ap.parse_args()
@@ -373,7 +384,7 @@ def main():
     plain_occ = [h[:, 1].view(torch.int32).ne(-1).sum().item() for h in hits]
 
     # ---- batched: autotuned sort threshold / block size / stack depth, CUDA graph
-    cache = str(ROOT / "profiles" / "autotune_cache.txt") if os.environ.get("RQ_TUNE_CACHE") else None
+    cache = os.environ.get("RQ_TUNE_CACHE") or None  # a file path chosen by the caller, e.g. under /tmp
     t0 = time.time()
     bp = rq.autotune_batch(ctx, items, rq.ANY, cache_path=cache, stream=stream)
     log(f"[bench] autotune {time.time()-t0:.1f}s -> block {bp.launch.block_size} smem {bp.launch.smem_stack} "
@@ -455,7 +466,8 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     achieved = alg_bytes / (ms_kernel * 1e-3) / 1e9
     traffic = profile_traffic(args.workload + ("_quick" if args.quick else ""))
-    l2_gbs = measure_l2_read(stream)
+    l2 = measure_l2_read(stream)
+    l2_gbs = l2["peak"]
     link = measure_link()
     link_ms = link_bound_ms(total_rays * 32, total_rays * 16, link)
 
@@ -508,6 +520,26 @@ def main():
         serving = run_serving()
         log(f"[bench] serving {time.time()-t0:.1f}s")
 
+    # ---- where batching gains over plain launches: per-scene plain launch
+    # times against the batch's rate, and a regime of many small items
+    batching = None
+    if args.workload == "batched" and not args.quick and world == 1:
+        t0 = time.time()
+        batching = batching_breakdown(ctx, scenes, rays, hits, ms_batch, stream, warmup)
+        batching["small_items"] = batching_small_items(ctx, stream, warmup, args.steps)
+        log(f"[bench] batching breakdown {time.time()-t0:.1f}s")
+
+    # ---- the other single-GPU configurations, each in its own process (so
+    # their buffers do not share the device with this one's): the plain small
+    # scene, the city and the 30M-triangle scene, with their own rooflines
+    configs = None
+    if args.workload == "batched" and not args.quick and world == 1 and not args.no_configs:
+        t0 = time.time()
+        configs = {"config0_plain_small": run_config_process("small", args, warmup),
+                   "config1_city": run_config_process("city", args, warmup),
+                   "config2_large": run_config_process("large", args, warmup)}
+        log(f"[bench] configs 0-2 {time.time()-t0:.1f}s")
+
     # ---- CPU baseline (oracle restatement, all host threads, bounded sample)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -530,7 +562,10 @@ def main():
         "data": "synthetic (seeded procedural scenes and AO rays; the reference's mesh.dat/samplecache.dat are not shipped)",
         "config": {
             "workload": ("batched: 64 heightfield+box scenes, tris log-U[10k,2M], AO any-hit rays log-U[256K,8M], "
-                         "one persistent launch, Morton sort, CUDA graph, autotuned")
+                         "one persistent launch, " +
+                         ("Morton sort (threshold %d rays), " % bp.sort_threshold if bp.sort_threshold >= 0
+                          else "Morton sort off (autotuner), ") +
+                         ("CUDA graph, " if bp.use_graph else "") + "autotuned")
             if args.workload == "batched" and not args.quick else f"{args.workload}{' (quick)' if args.quick else ''}",
             "scenes": len(spec),
             "triangles": int(sum(s["tris"] for s in spec)),
@@ -569,14 +604,20 @@ def main():
                      "nodes_per_ray": round(nodes_total / total_rays, 3),
                      "tris_per_ray": round(tris_total / total_rays, 3),
                      "l2": {"peak": round(l2_gbs, 1), "frac": round(achieved / l2_gbs, 4),
-                            "peak_source": "rq_probe_l2_read: 48 MB L2-resident buffer, 16 B L1-bypassing loads, "
-                                           "measured in this run"}},
+                            "peak_source": "rq_probe_l2_read_shape: best of 24 shapes (8-48 MB L2-resident buffers, "
+                                           "coalesced 16 B L1-bypassing loads, SMs x 8/16/32 blocks, 4/8 loads in "
+                                           "flight), measured in this run",
+                            "best_shape": l2["best"]}},
         "gpu_launches": int(launches_per_step * args.steps),
         "clocks": clocks,
         "clocks_ms_per_step": round(ms_batch2, 4),
     }
     if serving is not None:
         line["serving"] = serving
+    if configs is not None:
+        line["configs"] = configs
+    if batching is not None:
+        line["batching"] = batching
     if kernels is not None:
         line["kernels"] = kernels
     if ref_gpu is not None:
@@ -885,6 +926,97 @@ def _counted_bytes(ctx, scene, rays, query, stream):
     return 48 * int(rays.shape[0]) + 80 * nodes + 48 * tris, nodes, tris
 
 
+def batching_breakdown(ctx, scenes, rays, hits, ms_batch: float, stream, warmup: int) -> dict:
+    """Each scene's plain launch timed alone (CUDA events) against the time
+    its rays take at the batch's overall rate; the difference is that
+    launch's tail (its last waves running with the GPU partly idle) plus its
+    launch overhead -- all that one persistent launch over every item can
+    remove.  Summed per quartile of the scenes' ray counts."""
+    import cwbvh_b200 as rq
+    total = sum(int(r.shape[0]) for r in rays)
+    rate = total / ms_batch  # rays per ms in the batch
+    rows = []
+    for ds, r, h in zip(scenes, rays, hits):
+        ms = time_steps(lambda: rq.trace(ctx, ds.scene, r, h, rq.ANY, stream=stream), 3, 1, stream)
+        rows.append((int(r.shape[0]), ds.n_tris, ms, ms - r.shape[0] / rate))
+    ctx.check(stream)
+    rows.sort()
+    q = []
+    for k in range(4):
+        part = rows[k * len(rows) // 4:(k + 1) * len(rows) // 4]
+        q.append({"scenes": len(part), "rays": [part[0][0], part[-1][0]],
+                  "triangles_mean": int(np.mean([p[1] for p in part])),
+                  "plain_ms": round(sum(p[2] for p in part), 3),
+                  "at_batch_rate_ms": round(sum(p[0] for p in part) / rate, 3),
+                  "tail_ms_per_launch": round(float(np.mean([p[3] for p in part])), 4)})
+    return {"per_quartile_of_rays": q, "plain_sum_ms": round(sum(p[2] for p in rows), 3),
+            "batched_ms": round(ms_batch, 3),
+            "tail_ms_per_launch_mean": round(float(np.mean([p[3] for p in rows])), 4),
+            "what": "each scene's plain launch timed alone vs its rays at the batch's rate; the difference is the "
+                    "launch's tail and overhead, which one persistent launch removes"}
+
+
+def batching_small_items(ctx, stream, warmup: int, steps: int, n_items: int = 64, n_rays: int = 256 * 1024) -> dict:
+    """Batching where it has most to remove: 64 small scenes (10k-20k
+    triangles, the low end of the batched configuration) with 256K AO rays
+    each, as 64 plain launches and as one batch launch (CUDA graph)."""
+    import torch
+    import cwbvh_b200 as rq
+    from cwbvh_b200 import workloads as W
+    rng = np.random.default_rng(99)
+    tris = np.exp(rng.uniform(math.log(10_000), math.log(20_000), n_items)).astype(np.int64)
+    items, keep = [], []
+    for k, t in enumerate(tris):
+        V, I = W.scene_of_size(500 + k, int(t))
+        ds = W.upload(V, I, rq.CWBVH)
+        r = W.ao_rays(ds, n_rays, seed=600 + k, stream=stream)
+        h = torch.empty((n_rays, 4), device="cuda")
+        items.append((ds.scene, r, h))
+        keep.append(ds)
+    torch.cuda.synchronize()
+
+    def plain():
+        for sc, r, h in items:
+            rq.trace(ctx, sc, r, h, rq.ANY, stream=stream)
+    ms_plain = time_steps(plain, steps, warmup, stream)
+    occ_plain = [int(h[:, 1].view(torch.int32).ne(-1).sum().item()) for _, _, h in items]
+    b = rq.Batch(ctx, items, rq.ANY, sort_threshold=-1, use_graph=True)
+    ms_batch = time_steps(lambda: b.run(stream), steps, warmup, stream)
+    ctx.check(stream)
+    occ_batch = [int(h[:, 1].view(torch.int32).ne(-1).sum().item()) for _, _, h in items]
+    b.close()
+    total = n_items * n_rays
+    return {"scenes": n_items, "triangles": [int(tris.min()), int(tris.max())], "rays_per_scene": n_rays,
+            "plain_mrays_per_s": round(total / ms_plain / 1e3, 1), "batched_mrays_per_s": round(total / ms_batch / 1e3, 1),
+            "batched_vs_plain": round(ms_plain / ms_batch, 3), "occlusion_identical": occ_plain == occ_batch}
+
+
+def run_config_process(workload: str, args, warmup: int, timeout_s: int = 900) -> dict:
+    """One configuration's bench line from `bench.py --workload <workload>`
+    in a child process on the same GPU (no CPU baseline there: the CPU figure
+    is the default line's), minus the keys the parent line already carries."""
+    cmd = [sys.executable, str(ROOT / "bench.py"), "--workload", workload, "--steps", str(args.steps),
+           "--warmup", str(warmup), "--no-cpu"]
+    if args.no_ref_gpu:
+        cmd.append("--no-ref-gpu")
+    env = dict(os.environ)
+    for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "LOCAL_WORLD_SIZE"):
+        env.pop(k, None)
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env, cwd=str(ROOT))
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"bench.py --workload {workload} exceeded {timeout_s}s"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr or "").strip().splitlines()[-1:] or ["no output"]
+        return {"unavailable": f"bench.py --workload {workload} exited {r.returncode}: {tail[0][:300]}"}
+    d = json.loads(lines[-1])
+    for k in ("metric", "n_gpus", "higher_is_better", "scaling", "vs_baseline", "data", "dtype", "steps", "warmup"):
+        d.pop(k, None)
+    d["command"] = " ".join(["python", "bench.py"] + cmd[2:])
+    return d
+
+
 def _pass(name, n_rays, ms, alg=None, peak=None, l2=None):
     d = {"rays": int(n_rays), "ms": round(ms, 4), "mrays_per_s": round(n_rays / (ms * 1e-3) / 1e6, 2)}
     if alg is not None:
@@ -960,7 +1092,7 @@ def run_city(args, world, rank, dist):
     occ = float((ah[:, 1].view(torch.int32) != -1).float().mean().item())
     same = bool(torch.equal(ah[:, 1].view(torch.int32) != -1, sah[:, 1].view(torch.int32) != -1))
     peak, peak_kind = measured_peak_hbm()
-    l2 = measure_l2_read(stream)
+    l2 = measure_l2_read(stream)["peak"]
     a_prim = _counted_bytes(ctx, sc, prim, rq.CLOSEST, stream)
     a_ao = _counted_bytes(ctx, sc, ao, rq.ANY, stream)
     ref = {}
@@ -1179,7 +1311,7 @@ def run_large(args, world, rank, dist):
     occ = float((hits[:, 1].view(torch.int32) != -1).float().mean().item())
     fused_same = bool(torch.equal(occl, (hits[:, 1].view(torch.int32) != -1).view(-1, spp).sum(1, dtype=torch.int32)))
     peak, peak_kind = measured_peak_hbm()
-    l2 = measure_l2_read(stream)
+    l2 = measure_l2_read(stream)["peak"]
     alg = _counted_bytes(ctx, sc, rays, rq.ANY, stream)
     unsorted = _pass("unsorted", n, ms_plain, alg, peak, l2)
     best = min(ms_plain, ms_sorted, ms_fused)

@@ -74,6 +74,11 @@ class RequestStats(C.Structure):
                 ("batch_id", i32), ("status", i32)]
 
 
+class ServerMemoryStats(C.Structure):
+    _fields_ = [("pool_bytes", i64), ("in_use_bytes", i64), ("peak_in_use_bytes", i64), ("admission_waits", i64),
+                ("pieces", i64), ("max_batch_rays", i64)]
+
+
 def _sig(name, res, *args):
     fn = getattr(lib, name)
     fn.restype = res
@@ -121,6 +126,7 @@ _sig("rq_server_submit", C.c_int, vp, i32, vp, vp, i64, P(u64))
 _sig("rq_server_wait", C.c_int, vp, u64, i64, P(RequestStats))
 _sig("rq_server_cancel", C.c_int, vp, u64)
 _sig("rq_server_destroy", C.c_int, vp)
+_sig("rq_server_memory", C.c_int, vp, P(ServerMemoryStats))
 _sig("rq_gen_heightfield_boxes", C.c_int, u64, C.c_int, C.c_int, f32, f32, P(vp), P(i64), P(vp), P(i64))
 _sig("rq_gen_city", C.c_int, u64, C.c_int, P(vp), P(i64), P(vp), P(i64))
 _sig("rq_gen_spheres_terrain", C.c_int, u64, i64, P(vp), P(i64), P(vp), P(i64))
@@ -152,6 +158,7 @@ _sig("rq_camera_rays", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, f32, f32, vp,
 _sig("rq_camera_rays_tiled", C.c_int, vp, vp, vp, f32, C.c_int, C.c_int, C.c_int, C.c_int, f32, f32, vp, vp)
 _sig("rq_surfels_from_hits", C.c_int, vp, vp, vp, i64, vp, vp, vp, vp)
 _sig("rq_probe_l2_read", C.c_int, vp, i64, C.c_int, vp, vp)
+_sig("rq_probe_l2_read_shape", C.c_int, vp, i64, C.c_int, C.c_int, C.c_int, vp, vp)
 _sig("rq_trace_ao", C.c_int, vp, vp, vp, i64, C.c_int, vp, P(Launch), vp)
 # instancing
 _sig("rq_tlas_create", C.c_int, P(vp), C.c_int, vp, vp, i64, P(vp))
@@ -159,6 +166,11 @@ _sig("rq_tlas_destroy", C.c_int, vp)
 _sig("rq_tlas_buffers", C.c_int, vp, P(vp), P(i64), P(vp), P(i64), P(vp))
 _sig("rq_trace_instanced", C.c_int, vp, vp, vp, vp, vp, i64, C.c_int, P(Launch), vp)
 _sig("rq_tlas_build_host", C.c_int, vp, C.c_int, vp, vp, i64, P(vp))
+# one ray set over several devices
+_sig("rq_shard_range", C.c_int, i64, C.c_int, C.c_int, P(i64), P(i64))
+_sig("rq_sharded_create", C.c_int, C.c_int, vp, vp, i64, P(vp))
+_sig("rq_sharded_trace", C.c_int, vp, vp, vp, i64, C.c_int, P(Launch), vp)
+_sig("rq_sharded_destroy", C.c_int, vp)
 # serving
 _sig("rq_server_submit_bake", C.c_int, vp, i32, vp, vp, vp, i64, C.c_int, u64, f32, f32, f32, vp, P(u64))
 
