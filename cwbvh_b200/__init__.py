@@ -22,6 +22,7 @@ from ._native import ANY, BVH2, CLOSEST, CWBVH, Launch, RQError, check, lib
 
 GPU_BUILD_LBVH = 0  # rq_build_scene_gpu: Karras radix tree over the Morton order
 GPU_BUILD_PLOC = 1  # rq_build_scene_gpu: parallel locally-ordered clustering
+GPU_BUILD_THREAD_TREELETS = 0x100  # OR-ed into the method: one thread per treelet (same trees, slower)
 
 __all__ = [
     "ANY", "BVH2", "CLOSEST", "CWBVH", "GPU_BUILD_LBVH", "GPU_BUILD_PLOC", "Launch", "RQError", "HostBVH", "Scene", "Context", "Batch", "Server",
@@ -390,6 +391,46 @@ def trace_ordered(ctx: Context, scene: Scene, rays, hits, query: int = ANY, stre
                                _stream(stream)), "rq_trace_ordered")
 
 
+def shard_range(count: int, n_parts: int, part: int):
+    """(begin, size) of ray range `part` of `count` over `n_parts` (rq_shard_range)."""
+    b, m = C.c_int64(), C.c_int64()
+    check(lib.rq_shard_range(count, n_parts, part, C.byref(b), C.byref(m)), "rq_shard_range")
+    return b.value, m.value
+
+
+class Sharded:
+    """One ray set over several devices holding replicas of one scene
+    (rq_sharded_*): contiguous ray ranges per device, hits gathered into the
+    caller's buffer on the first device by peer copies."""
+
+    def __init__(self, devices: Sequence[int], scenes: Sequence["Scene"], max_rays: int):
+        if len(devices) != len(scenes) or not devices:
+            raise ValueError("one scene per device")
+        self._scenes = list(scenes)
+        devs = (C.c_int * len(devices))(*devices)
+        hs = (C.c_void_p * len(scenes))(*[sc._h.value if isinstance(sc._h, C.c_void_p) else sc._h for sc in scenes])
+        h = C.c_void_p()
+        check(lib.rq_sharded_create(len(devices), devs, hs, max_rays, C.byref(h)), "rq_sharded_create")
+        self._h = h
+
+    def trace(self, rays, hits, query: int = ANY, launch: Optional[Launch] = None, stream=None) -> None:
+        n = _rows(rays, 8, "rays")
+        check(lib.rq_sharded_trace(self._h, _ptr(rays), _ptr(hits), n, query,
+                                   C.byref(launch) if launch is not None else None, _stream(stream)),
+              "rq_sharded_trace")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib.rq_sharded_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Tlas:
     """Instances of CWBVH scenes under a top-level CWBVH (rq_tlas_*).
 
@@ -679,6 +720,13 @@ class Server:
 
     def cancel(self, ticket: int) -> int:
         return int(lib.rq_server_cancel(self._h, ticket))
+
+    def memory(self) -> dict:
+        """Pool accounting (rq_server_memory): pool, in-use and peak bytes,
+        admission waits, pieces queued, rays per launch."""
+        m = N.ServerMemoryStats()
+        check(lib.rq_server_memory(self._h, C.byref(m)), "rq_server_memory")
+        return {f: getattr(m, f) for f, _ in N.ServerMemoryStats._fields_}
 
     def close(self) -> None:
         # `lib` is None once the interpreter is tearing modules down; the
