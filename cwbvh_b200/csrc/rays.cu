@@ -46,10 +46,13 @@ __device__ inline float3 norm3(float3 a) { return mul3(a, 1.0f / len3(a)); }
 // One ray per (surfel, sample), surfel = i / spp: tangent frame from n x z
 // (n x y when that is short), concentric disk lifted to the cosine
 // hemisphere, origin pushed off the surface by radius * offset_scale
-// (src/ValidationKernels.cu:41-101).
+// (src/ValidationKernels.cu:41-101).  The random stream of ray i is keyed by
+// its index first_ray + i in the whole request, so a request generated in
+// pieces gives the same rays as in one call.
 __global__ void aorays_kernel(const float4* __restrict__ pos, const float4* __restrict__ nrm,
-                              const float* __restrict__ radius, int64_t n_rays, int spp, uint32_t k0, uint32_t k1,
-                              float tmin, float tmax, float offset_scale, Ray* __restrict__ out) {
+                              const float* __restrict__ radius, int64_t n_rays, int spp, int64_t first_ray,
+                              uint32_t k0, uint32_t k1, float tmin, float tmax, float offset_scale,
+                              Ray* __restrict__ out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_rays) return;
     const int64_t s = i / spp;
@@ -65,7 +68,8 @@ __global__ void aorays_kernel(const float4* __restrict__ pos, const float4* __re
     if (len3(t1) < 0.1f) t1 = cross3(n, make_float3(0.f, 1.f, 0.f));
     t1 = norm3(t1);
     const float3 t2 = norm3(cross3(t1, n));
-    const U4 rnd = philox4x32_10(U4{(uint32_t)i, (uint32_t)((uint64_t)i >> 32), 0u, 0u}, k0, k1);
+    const uint64_t ctr = (uint64_t)(first_ray + i);
+    const U4 rnd = philox4x32_10(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u}, k0, k1);
     const float a = 2.0f * unit24(rnd.x) - 1.0f, b = 2.0f * unit24(rnd.y) - 1.0f;
     float dxl = 0.f, dyl = 0.f;
     if (a != 0.f || b != 0.f) {
@@ -218,6 +222,20 @@ __global__ void gather_rays_kernel(const TraceItem* __restrict__ items, const ui
 
 static unsigned blocks_for(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
+rq_status aorays_launch(const float* pos, const float* nrm, const float* radius, int64_t n_surfels, int spp,
+                        int64_t first_ray, uint64_t seed, float tmin, float tmax, float offset_scale, rq_ray* out_rays,
+                        void* stream) {
+    if (n_surfels < 0 || spp <= 0 || first_ray < 0 || (n_surfels > 0 && (!pos || !nrm || !out_rays)))
+        return RQ_ERR_INVALID_ARG;
+    const int64_t n = n_surfels * spp;
+    if (n == 0) return RQ_OK;
+    aorays_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const float4*)pos, (const float4*)nrm, radius, n, spp, first_ray, (uint32_t)seed, (uint32_t)(seed >> 32),
+        tmin, tmax, offset_scale, (Ray*)out_rays);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
 rq_status sort_plan_create(const std::vector<TraceItem>& items, const std::vector<float>& bounds, SortPlan& plan) {
     plan = SortPlan();
     plan.n_items = (int)items.size();
@@ -304,14 +322,7 @@ extern "C" {
 
 rq_status rq_aorays(const float* pos, const float* nrm, const float* radius, int64_t n_surfels, int spp, uint64_t seed,
                     float tmin, float tmax, float offset_scale, rq_ray* out_rays, void* stream) {
-    if (n_surfels < 0 || spp <= 0 || (n_surfels > 0 && (!pos || !nrm || !out_rays))) return RQ_ERR_INVALID_ARG;
-    const int64_t n = n_surfels * spp;
-    if (n == 0) return RQ_OK;
-    aorays_kernel<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
-        (const float4*)pos, (const float4*)nrm, radius, n, spp, (uint32_t)seed, (uint32_t)(seed >> 32), tmin, tmax,
-        offset_scale, (Ray*)out_rays);
-    RQ_CUDA(cudaGetLastError());
-    return RQ_OK;
+    return rq::aorays_launch(pos, nrm, radius, n_surfels, spp, 0, seed, tmin, tmax, offset_scale, out_rays, stream);
 }
 
 rq_status rq_sample_surfels(const float* vertices, const int32_t* indices, int64_t nt, int64_t n_surfels,

@@ -59,6 +59,12 @@ rq_status reset_counter(rq_ctx* ctx, cudaStream_t s);
 TraceItem scene_item(const rq_scene* sc, const rq_ray* rays, rq_hit* hits, int64_t count);
 TraceParams base_params(rq_ctx* ctx, const rq_launch& l);
 
+// AO rays of n_surfels surfels (rays.cu); ray k of the call is ray
+// first_ray + k of the request it belongs to (its random stream).
+rq_status aorays_launch(const float* pos, const float* nrm, const float* radius, int64_t n_surfels, int spp,
+                        int64_t first_ray, uint64_t seed, float tmin, float tmax, float offset_scale, rq_ray* out_rays,
+                        void* stream);
+
 // Morton keys + radix sort of the rays of several items (rays.cu).
 struct SortPlan {
     int n_items = 0;

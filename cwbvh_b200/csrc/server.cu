@@ -4,20 +4,31 @@
 // host hit buffer); a bake request is (scene id, host surfels, rays per
 // surfel, host AO buffer): its rays are generated on the device and its
 // occluded rays counted per surfel in the trace epilogue, so only the surfels
-// cross PCIe in and one float per surfel comes back.  A dispatcher thread
-// owns `streams` workers; each worker has one device arena of max_batch_rays
-// x 48 B, so the HBM taken by request buffers never exceeds
-// streams x max_batch_rays x 48 <= hbm_budget_bytes.  Whenever a worker is
-// free, the dispatcher admits the oldest queued requests whose buffers fit
-// its arena, copies their inputs in, traces all of them in one persistent
-// batch launch and copies the results back -- all on the worker's stream --
-// so batches on different workers overlap on the device (the next batch's
-// blocks start as the previous one drains) and copies overlap traces.
-// Requests arriving meanwhile are admitted into the next free worker.
+// cross PCIe in and one float per surfel comes back.
+//
+// Memory.  The HBM budget is one device pool, allocated when the server is
+// created; every request buffer lives in it.  A request is cut into pieces
+// of at most max_batch_rays rays (whole surfels for bake requests) that each
+// fit the pool, so no request is refused for its size: pieces of one request
+// may run in different launches, and the request completes when its last
+// piece has.  Admission is by bytes: a piece is admitted when the pool can
+// give it its buffers (first fit, 256-B aligned), and gives them back when
+// its launch has finished, so the bytes in use never exceed the budget and
+// queued pieces wait while the budget is taken.
+//
+// Launches.  A dispatcher thread owns `streams` workers.  Whenever a worker
+// is free, it admits the oldest queued pieces (arrival order, up to
+// max_batch_rays rays in all) whose buffers the pool can give, copies their
+// inputs in, traces all of them in one persistent batch launch and copies the
+// results back -- all on the worker's stream -- so batches on different
+// workers overlap on the device (the next batch's blocks start as the
+// previous one drains) and copies overlap traces.  Pieces arriving meanwhile
+// are admitted into the next free worker.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -59,14 +70,76 @@ struct Req {
     float tmin = 0.f, tmax = 0.f, offset_scale = 0.f;
     // result: hits (ray request) or AO per surfel (bake request)
     void* host_out = nullptr;
-    void* dev_out = nullptr;
-    int64_t out_bytes = 0;
-    int64_t arena_bytes = 0;     // device bytes the request occupies while running
+    bool deferred_copy = false;  // pageable destination: copied after the stream finishes
+    int pieces_left = 0;
+    int pieces_started = 0;
     double submit_ms = 0, start_ms = 0, done_ms = 0;
-    int32_t batch = -1;
+    int32_t batch = -1;          // launch of the request's first piece
     rq_status status = RQ_OK;
     enum State { kQueued, kRunning, kDone } state = kQueued;
-    bool deferred_copy = false;  // pageable destination: copied after the stream finishes
+};
+
+// A contiguous part of a request: rays [first, first + n) of a ray request,
+// or surfels [first, first + n) of a bake request.
+struct Piece {
+    Req* req = nullptr;
+    int64_t first = 0;
+    int64_t n = 0;
+    int64_t rays = 0;        // rays traced
+    int64_t bytes = 0;       // pool bytes while admitted
+    int64_t off = -1;        // pool offset while admitted
+    void* dev_out = nullptr;
+};
+
+int64_t ray_piece_bytes(int64_t n) {
+    return align256(n * (int64_t)sizeof(rq::Ray)) + align256(n * (int64_t)sizeof(rq::Hit));
+}
+int64_t bake_piece_bytes(int64_t n, int spp, bool radius) {
+    return 2 * align256(16 * n) + (radius ? align256(4 * n) : 0) + align256(4 * n) +
+           align256(n * spp * (int64_t)sizeof(rq::Ray));
+}
+
+// First-fit allocator over the server's device pool (offsets, 256-B units).
+struct Pool {
+    char* base = nullptr;
+    int64_t size = 0;
+    std::map<int64_t, int64_t> free_;  // offset -> length
+    int64_t in_use = 0, peak = 0;
+
+    void reset(char* b, int64_t n) {
+        base = b;
+        size = n;
+        free_.clear();
+        if (n > 0) free_[0] = n;
+    }
+    int64_t alloc(int64_t n) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            const int64_t off = it->first, len = it->second;
+            free_.erase(it);
+            if (len > n) free_[off + n] = len - n;
+            in_use += n;
+            peak = std::max(peak, in_use);
+            return off;
+        }
+        return -1;
+    }
+    void release(int64_t off, int64_t n) {
+        in_use -= n;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
 };
 
 // Occluded-ray counts of a bake request turned into AO fractions in place.
@@ -78,10 +151,9 @@ __global__ void counts_to_ao_kernel(uint32_t* counts, int64_t n, int spp) {
 struct Worker {
     cudaStream_t stream = nullptr;
     rq_ctx* ctx = nullptr;
-    char* d_arena = nullptr;
     rq::TraceItem* d_items = nullptr;
     rq::TraceItem* h_items = nullptr;  // pinned
-    std::vector<Req*> inflight;
+    std::vector<Piece*> inflight;
     bool busy = false;
     bool finished = false;  // set by the stream callback
 };
@@ -92,15 +164,18 @@ constexpr int kMaxItems = 4096;
 
 struct rq_server {
     rq_server_params params{};
-    int64_t cap = 0;          // rays of a ray request that fill an arena
-    int64_t arena_bytes = 0;  // per worker
+    int64_t cap = 0;          // rays per launch (and per piece)
+    char* d_pool = nullptr;
+    Pool pool;
+    int64_t admission_waits = 0;  // times the oldest queued piece waited for pool bytes
+    int64_t pieces_total = 0;
     rq_launch launch{};
     rq_bvh_kind kind = RQ_BVH_CWBVH;
     std::vector<rq_scene*> scenes;
     std::mutex mu;
     std::condition_variable cv;       // dispatcher wake-ups
     std::condition_variable cv_done;  // request completions
-    std::deque<Req*> pending;
+    std::deque<Piece*> pending;
     std::unordered_map<uint64_t, Req*> reqs;
     uint64_t next_ticket = 1;
     int32_t next_batch = 0;
@@ -110,7 +185,7 @@ struct rq_server {
     rq_status fatal = RQ_OK;
 
     void run();
-    void launch_batch(Worker& w, std::vector<Req*>& batch, int32_t batch_id);
+    void launch_batch(Worker& w, std::vector<Piece*>& batch, int32_t batch_id);
     void finalize(Worker& w);
 };
 
@@ -124,54 +199,58 @@ static void CUDART_CB worker_done(void* user) {
     delete pair;
 }
 
-void rq_server::launch_batch(Worker& w, std::vector<Req*>& batch, int32_t batch_id) {
+void rq_server::launch_batch(Worker& w, std::vector<Piece*>& batch, int32_t batch_id) {
     rq_status st = RQ_OK;
     auto ok = [&](cudaError_t e) {
         if (e != cudaSuccess && st == RQ_OK) st = rq::cuda_fail(e, "rq_server batch");
     };
-    int64_t off = 0, ray_begin = 0;
+    int64_t ray_begin = 0;
     for (size_t k = 0; k < batch.size(); ++k) {
-        Req* r = batch[k];
-        r->batch = batch_id;
+        Piece* pc = batch[k];
+        Req* r = pc->req;
+        char* base = d_pool + pc->off;
+        int64_t off = 0;
         rq::TraceItem it;
         if (!r->bake) {
-            rq::Ray* d_rays = reinterpret_cast<rq::Ray*>(w.d_arena + off);
-            off += align256(r->count * (int64_t)sizeof(rq::Ray));
-            rq::Hit* d_hits = reinterpret_cast<rq::Hit*>(w.d_arena + off);
-            off += align256(r->count * (int64_t)sizeof(rq::Hit));
-            ok(cudaMemcpyAsync(d_rays, r->host_rays, (size_t)r->count * sizeof(rq::Ray), cudaMemcpyHostToDevice,
-                               w.stream));
-            it = rq::scene_item(scenes[r->scene], (const rq_ray*)d_rays, (rq_hit*)d_hits, r->count);
-            r->dev_out = d_hits;
+            rq::Ray* d_rays = reinterpret_cast<rq::Ray*>(base + off);
+            off += align256(pc->n * (int64_t)sizeof(rq::Ray));
+            rq::Hit* d_hits = reinterpret_cast<rq::Hit*>(base + off);
+            ok(cudaMemcpyAsync(d_rays, r->host_rays + pc->first, (size_t)pc->n * sizeof(rq::Ray),
+                               cudaMemcpyHostToDevice, w.stream));
+            it = rq::scene_item(scenes[r->scene], (const rq_ray*)d_rays, (rq_hit*)d_hits, pc->n);
+            pc->dev_out = d_hits;
         } else {
-            const int64_t n = r->n_surfels;
-            float* d_pos = reinterpret_cast<float*>(w.d_arena + off);
+            const int64_t n = pc->n;
+            float* d_pos = reinterpret_cast<float*>(base + off);
             off += align256(16 * n);
-            float* d_nrm = reinterpret_cast<float*>(w.d_arena + off);
+            float* d_nrm = reinterpret_cast<float*>(base + off);
             off += align256(16 * n);
             float* d_rad = nullptr;
             if (r->host_radius) {
-                d_rad = reinterpret_cast<float*>(w.d_arena + off);
+                d_rad = reinterpret_cast<float*>(base + off);
                 off += align256(4 * n);
             }
-            uint32_t* d_counts = reinterpret_cast<uint32_t*>(w.d_arena + off);
+            uint32_t* d_counts = reinterpret_cast<uint32_t*>(base + off);
             off += align256(4 * n);
-            rq_ray* d_rays = reinterpret_cast<rq_ray*>(w.d_arena + off);
-            off += align256(r->count * (int64_t)sizeof(rq::Ray));
-            ok(cudaMemcpyAsync(d_pos, r->host_pos, (size_t)(16 * n), cudaMemcpyHostToDevice, w.stream));
-            ok(cudaMemcpyAsync(d_nrm, r->host_nrm, (size_t)(16 * n), cudaMemcpyHostToDevice, w.stream));
-            if (d_rad) ok(cudaMemcpyAsync(d_rad, r->host_radius, (size_t)(4 * n), cudaMemcpyHostToDevice, w.stream));
+            rq_ray* d_rays = reinterpret_cast<rq_ray*>(base + off);
+            ok(cudaMemcpyAsync(d_pos, r->host_pos + 4 * pc->first, (size_t)(16 * n), cudaMemcpyHostToDevice,
+                               w.stream));
+            ok(cudaMemcpyAsync(d_nrm, r->host_nrm + 4 * pc->first, (size_t)(16 * n), cudaMemcpyHostToDevice,
+                               w.stream));
+            if (d_rad)
+                ok(cudaMemcpyAsync(d_rad, r->host_radius + pc->first, (size_t)(4 * n), cudaMemcpyHostToDevice,
+                                   w.stream));
             ok(cudaMemsetAsync(d_counts, 0, (size_t)(4 * n), w.stream));
             if (st == RQ_OK)
-                st = rq_aorays(d_pos, d_nrm, d_rad, n, r->spp, r->seed, r->tmin, r->tmax, r->offset_scale, d_rays,
-                               w.stream);
-            it = rq::scene_item(scenes[r->scene], d_rays, nullptr, r->count);
+                st = rq::aorays_launch(d_pos, d_nrm, d_rad, n, r->spp, pc->first * r->spp, r->seed, r->tmin, r->tmax,
+                                       r->offset_scale, d_rays, w.stream);
+            it = rq::scene_item(scenes[r->scene], d_rays, nullptr, pc->rays);
             it.ao_counts = d_counts;
             it.ao_spp = r->spp;
-            r->dev_out = d_counts;
+            pc->dev_out = d_counts;
         }
         it.ray_begin = ray_begin;
-        ray_begin += r->count;
+        ray_begin += pc->rays;
         w.h_items[k] = it;
     }
     if (st == RQ_OK)
@@ -186,17 +265,23 @@ void rq_server::launch_batch(Worker& w, std::vector<Req*>& batch, int32_t batch_
         p.total_rays = ray_begin;
         st = rq::launch_trace(kind, params.query, launch, true, false, p, w.stream);
     }
-    for (Req* r : batch) {
+    for (Piece* pc : batch) {
+        Req* r = pc->req;
         if (r->bake && st == RQ_OK) {
-            counts_to_ao_kernel<<<(unsigned)((r->n_surfels + 255) / 256), 256, 0, w.stream>>>(
-                (uint32_t*)r->dev_out, r->n_surfels, r->spp);
+            counts_to_ao_kernel<<<(unsigned)((pc->n + 255) / 256), 256, 0, w.stream>>>((uint32_t*)pc->dev_out, pc->n,
+                                                                                       r->spp);
             ok(cudaGetLastError());
         }
-        r->deferred_copy = !is_pinned(r->host_out);
+        const int64_t out_elem = r->bake ? 4 : (int64_t)sizeof(rq::Hit);
         if (st == RQ_OK && !r->deferred_copy)
-            ok(cudaMemcpyAsync(r->host_out, r->dev_out, (size_t)r->out_bytes, cudaMemcpyDeviceToHost, w.stream));
+            ok(cudaMemcpyAsync(static_cast<char*>(r->host_out) + pc->first * out_elem, pc->dev_out,
+                               (size_t)(pc->n * out_elem), cudaMemcpyDeviceToHost, w.stream));
     }
-    for (Req* r : batch) r->status = st;
+    if (st != RQ_OK) {
+        std::lock_guard<std::mutex> lk(mu);
+        for (Piece* pc : batch)
+            if (pc->req->status == RQ_OK) pc->req->status = st;
+    }
     w.inflight = batch;
     w.finished = false;
     auto* pair = new std::pair<rq_server*, Worker*>(this, &w);
@@ -210,19 +295,30 @@ void rq_server::launch_batch(Worker& w, std::vector<Req*>& batch, int32_t batch_
 
 void rq_server::finalize(Worker& w) {
     // Called without the lock; the stream has completed.
-    rq_status kst = rq_ctx_check(w.ctx, w.stream);
-    for (Req* r : w.inflight) {
-        if (r->status == RQ_OK && r->deferred_copy &&
-            cudaMemcpy(r->host_out, r->dev_out, (size_t)r->out_bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-            r->status = RQ_ERR_CUDA;
-        if (r->status == RQ_OK) r->status = kst;
+    const rq_status kst = rq_ctx_check(w.ctx, w.stream);
+    std::vector<rq_status> copy_st(w.inflight.size(), RQ_OK);
+    for (size_t k = 0; k < w.inflight.size(); ++k) {
+        Piece* pc = w.inflight[k];
+        Req* r = pc->req;
+        const int64_t out_elem = r->bake ? 4 : (int64_t)sizeof(rq::Hit);
+        if (r->deferred_copy &&
+            cudaMemcpy(static_cast<char*>(r->host_out) + pc->first * out_elem, pc->dev_out,
+                       (size_t)(pc->n * out_elem), cudaMemcpyDeviceToHost) != cudaSuccess)
+            copy_st[k] = rq::cuda_fail(cudaGetLastError(), "rq_server: result copy");
     }
     const double t = now_ms();
     {
         std::lock_guard<std::mutex> lk(mu);
-        for (Req* r : w.inflight) {
-            r->done_ms = t;
-            r->state = Req::kDone;
+        for (size_t k = 0; k < w.inflight.size(); ++k) {
+            Piece* pc = w.inflight[k];
+            Req* r = pc->req;
+            pool.release(pc->off, pc->bytes);
+            if (r->status == RQ_OK) r->status = copy_st[k] != RQ_OK ? copy_st[k] : kst;
+            if (--r->pieces_left == 0) {
+                r->done_ms = t;
+                r->state = Req::kDone;
+            }
+            delete pc;
         }
         w.inflight.clear();
         w.busy = false;
@@ -234,22 +330,24 @@ void rq_server::finalize(Worker& w) {
 
 void rq_server::run() {
     std::unique_lock<std::mutex> lk(mu);
+    bool blocked = false;  // the oldest queued piece waits for pool bytes
     for (;;) {
         cv.wait(lk, [&] {
             bool any_busy = false;
             for (auto& w : workers) {
                 if (w.busy && w.finished) return true;
-                if (!stop && !w.busy && !pending.empty()) return true;
+                if (!stop && !w.busy && !pending.empty() && !blocked) return true;
                 any_busy |= w.busy;
             }
             return stop && !any_busy;
         });
-        // Completed batches first: they free arenas for the queue.
+        // Completed batches first: they give their bytes back to the pool.
         for (auto& w : workers)
             if (w.busy && w.finished) {
                 lk.unlock();
                 finalize(w);
                 lk.lock();
+                blocked = false;
             }
         if (stop) {
             bool any_busy = false;
@@ -258,24 +356,36 @@ void rq_server::run() {
             continue;  // wait for the in-flight batches to complete
         }
         for (auto& w : workers) {
-            if (w.busy || pending.empty()) continue;
-            std::vector<Req*> batch;
-            int64_t bytes = 0;
-            while (!pending.empty() && (int)batch.size() < kMaxItems &&
-                   bytes + pending.front()->arena_bytes <= arena_bytes) {
-                Req* r = pending.front();
+            if (w.busy || pending.empty() || blocked) continue;
+            std::vector<Piece*> batch;
+            int64_t rays = 0;
+            while (!pending.empty() && (int)batch.size() < kMaxItems) {
+                Piece* pc = pending.front();
+                if (!batch.empty() && rays + pc->rays > cap) break;
+                const int64_t off = pool.alloc(pc->bytes);
+                if (off < 0) {
+                    // Arrival order is kept: later pieces wait behind this one.
+                    blocked = true;
+                    ++admission_waits;
+                    break;
+                }
+                pc->off = off;
                 pending.pop_front();
-                bytes += r->arena_bytes;
-                batch.push_back(r);
+                rays += pc->rays;
+                batch.push_back(pc);
             }
             if (batch.empty()) continue;
             const double t = now_ms();
-            for (Req* r : batch) {
-                r->state = Req::kRunning;
-                r->start_ms = t;
+            const int32_t id = next_batch++;
+            for (Piece* pc : batch) {
+                Req* r = pc->req;
+                if (r->pieces_started++ == 0) {
+                    r->state = Req::kRunning;
+                    r->start_ms = t;
+                    r->batch = id;
+                }
             }
             w.busy = true;
-            const int32_t id = next_batch++;
             lk.unlock();
             launch_batch(w, batch, id);
             lk.lock();
@@ -288,28 +398,34 @@ extern "C" {
 rq_status rq_server_create(const rq_server_params* params, rq_server_t* out) {
     if (!params || !out || params->hbm_budget_bytes <= 0) return RQ_ERR_INVALID_ARG;
     if (params->query != RQ_CLOSEST && params->query != RQ_ANY) return RQ_ERR_INVALID_ARG;
+    const int streams = params->streams > 0 ? params->streams : 3;
+    const int64_t budget = params->hbm_budget_bytes / 256 * 256;
+    // Rays per launch: by default every worker can hold a full launch at
+    // once; never more than one piece of that size fits the pool.
+    int64_t cap = budget / (48 * (int64_t)streams);
+    if (params->max_batch_rays > 0) cap = params->max_batch_rays;
+    cap = std::min(cap, (budget - 512) / 48);
+    if (cap <= 0) return RQ_ERR_INVALID_ARG;
     rq_server* s = new rq_server();
     s->params = *params;
-    const int streams = params->streams > 0 ? params->streams : 3;
     s->params.streams = streams;
-    int64_t cap = params->hbm_budget_bytes / (48 * (int64_t)streams);
-    if (params->max_batch_rays > 0) cap = std::min(cap, params->max_batch_rays);
+    s->params.hbm_budget_bytes = budget;
     s->cap = cap;
-    s->arena_bytes = 48 * cap + 512;  // + two 256-B alignment pads: a ray request of `cap` rays fits
-    if (cap <= 0) {
+    cudaError_t e = cudaMalloc(&s->d_pool, (size_t)budget);
+    if (e != cudaSuccess) {
         delete s;
-        return RQ_ERR_INVALID_ARG;
+        return rq::cuda_fail(e, "rq_server_create: the HBM budget's pool");
     }
+    s->pool.reset(s->d_pool, budget);
     s->workers.resize(streams);
     rq_status st = RQ_OK;
     for (auto& w : s->workers) {
         if (st != RQ_OK) break;
-        cudaError_t e = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking);
+        e = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) st = rq_ctx_create(&w.ctx);
         else st = rq::cuda_fail(e, "rq_server_create");
         if (st != RQ_OK) break;
-        e = cudaMalloc(&w.d_arena, (size_t)s->arena_bytes);
-        if (e == cudaSuccess) e = cudaMalloc(&w.d_items, kMaxItems * sizeof(rq::TraceItem));
+        e = cudaMalloc(&w.d_items, kMaxItems * sizeof(rq::TraceItem));
         if (e == cudaSuccess) e = cudaMallocHost(&w.h_items, kMaxItems * sizeof(rq::TraceItem));
         if (e != cudaSuccess) st = rq::cuda_fail(e, "rq_server_create");
     }
@@ -336,22 +452,40 @@ rq_status rq_server_add_scene(rq_server_t s, rq_scene_t scene, int32_t* scene_id
     return RQ_OK;
 }
 
-static rq_status enqueue(rq_server_t s, Req* r, uint64_t* ticket) {
+// Cuts a request into pieces (each fits the pool and one launch) and queues
+// them in order.  `unit` is rays (ray request) or surfels (bake request).
+static rq_status enqueue(rq_server_t s, Req* r, int64_t units, int64_t units_per_piece) {
+    if (units_per_piece <= 0) {
+        delete r;
+        return RQ_ERR_BUDGET;
+    }
+    std::vector<Piece*> pieces;
+    for (int64_t first = 0; first < units; first += units_per_piece) {
+        Piece* pc = new Piece();
+        pc->req = r;
+        pc->first = first;
+        pc->n = std::min(units_per_piece, units - first);
+        pc->rays = r->bake ? pc->n * r->spp : pc->n;
+        pc->bytes = r->bake ? bake_piece_bytes(pc->n, r->spp, r->host_radius != nullptr) : ray_piece_bytes(pc->n);
+        pieces.push_back(pc);
+    }
+    r->pieces_left = (int)pieces.size();
+    r->deferred_copy = !is_pinned(r->host_out);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         rq_status st = RQ_OK;
         if (s->stop) st = RQ_ERR_CANCELLED;
         else if (r->scene < 0 || r->scene >= (int32_t)s->scenes.size()) st = RQ_ERR_NOT_FOUND;
-        else if (r->arena_bytes > s->arena_bytes) st = RQ_ERR_BUDGET;
         if (st != RQ_OK) {
+            for (Piece* pc : pieces) delete pc;
             delete r;
             return st;
         }
         r->ticket = s->next_ticket++;
         r->submit_ms = now_ms();
         s->reqs[r->ticket] = r;
-        s->pending.push_back(r);
-        *ticket = r->ticket;
+        for (Piece* pc : pieces) s->pending.push_back(pc);
+        s->pieces_total += (int64_t)pieces.size();
     }
     s->cv.notify_all();
     return RQ_OK;
@@ -365,9 +499,9 @@ rq_status rq_server_submit(rq_server_t s, int32_t scene_id, const rq_ray* host_r
     r->host_rays = host_rays;
     r->count = count;
     r->host_out = host_hits;
-    r->out_bytes = count * (int64_t)sizeof(rq::Hit);
-    r->arena_bytes = align256(count * (int64_t)sizeof(rq::Ray)) + align256(count * (int64_t)sizeof(rq::Hit));
-    return enqueue(s, r, ticket);
+    const rq_status st = enqueue(s, r, count, s->cap);
+    if (st == RQ_OK) *ticket = r->ticket;
+    return st;
 }
 
 rq_status rq_server_submit_bake(rq_server_t s, int32_t scene_id, const float* host_pos, const float* host_nrm,
@@ -391,10 +525,15 @@ rq_status rq_server_submit_bake(rq_server_t s, int32_t scene_id, const float* ho
     r->offset_scale = offset_scale;
     r->count = n_surfels * spp;
     r->host_out = host_ao;
-    r->out_bytes = 4 * n_surfels;
-    r->arena_bytes = 2 * align256(16 * n_surfels) + (host_radius ? align256(4 * n_surfels) : 0) +
-                     align256(4 * n_surfels) + align256(r->count * (int64_t)sizeof(rq::Ray));
-    return enqueue(s, r, ticket);
+    // Whole surfels per piece: at most one launch of rays, and buffers that
+    // fit the pool.
+    int64_t per = std::min<int64_t>(n_surfels, s->cap / spp);
+    const int64_t per_surfel = 40 + (host_radius ? 4 : 0) + 32 * (int64_t)spp;
+    per = std::min<int64_t>(per, (s->params.hbm_budget_bytes - 5 * 256) / per_surfel);
+    while (per > 0 && bake_piece_bytes(per, spp, host_radius != nullptr) > s->params.hbm_budget_bytes) --per;
+    const rq_status st = enqueue(s, r, n_surfels, per);
+    if (st == RQ_OK) *ticket = r->ticket;
+    return st;
 }
 
 rq_status rq_server_wait(rq_server_t s, uint64_t ticket, int64_t timeout_ms, rq_request_stats* stats) {
@@ -427,12 +566,34 @@ rq_status rq_server_cancel(rq_server_t s, uint64_t ticket) {
         auto it = s->reqs.find(ticket);
         if (it == s->reqs.end() || it->second->state != Req::kQueued) return RQ_ERR_NOT_FOUND;
         Req* r = it->second;
-        s->pending.erase(std::find(s->pending.begin(), s->pending.end(), r));
+        // Not started: all of its pieces are still queued.
+        for (auto p = s->pending.begin(); p != s->pending.end();) {
+            if ((*p)->req == r) {
+                delete *p;
+                p = s->pending.erase(p);
+            } else {
+                ++p;
+            }
+        }
+        r->pieces_left = 0;
         r->status = RQ_ERR_CANCELLED;
         r->state = Req::kDone;
         r->done_ms = now_ms();
     }
+    s->cv.notify_all();
     s->cv_done.notify_all();
+    return RQ_OK;
+}
+
+rq_status rq_server_memory(rq_server_t s, rq_server_memory_stats* out) {
+    if (!s || !out) return RQ_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    out->pool_bytes = s->pool.size;
+    out->in_use_bytes = s->pool.in_use;
+    out->peak_in_use_bytes = s->pool.peak;
+    out->admission_waits = s->admission_waits;
+    out->pieces = s->pieces_total;
+    out->max_batch_rays = s->cap;
     return RQ_OK;
 }
 
@@ -441,9 +602,15 @@ rq_status rq_server_destroy(rq_server_t s) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
-        for (Req* r : s->pending) {
+        const double t = now_ms();
+        for (Piece* pc : s->pending) {
+            Req* r = pc->req;
             r->status = RQ_ERR_CANCELLED;
-            r->state = Req::kDone;
+            if (--r->pieces_left == 0) {  // pieces still running finish it otherwise
+                r->state = Req::kDone;
+                r->done_ms = t;
+            }
+            delete pc;
         }
         s->pending.clear();
     }
@@ -453,11 +620,11 @@ rq_status rq_server_destroy(rq_server_t s) {
     for (auto& w : s->workers) {
         if (w.stream) cudaStreamSynchronize(w.stream);
         if (w.ctx) rq_ctx_destroy(w.ctx);
-        cudaFree(w.d_arena);
         cudaFree(w.d_items);
         if (w.h_items) cudaFreeHost(w.h_items);
         if (w.stream) cudaStreamDestroy(w.stream);
     }
+    cudaFree(s->d_pool);
     for (auto& kv : s->reqs) delete kv.second;
     delete s;
     return RQ_OK;

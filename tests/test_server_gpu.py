@@ -113,21 +113,18 @@ def test_results_match_plain_trace(rq, scenes):
 
 def test_failures_are_status_codes(rq, scenes):
     from cwbvh_b200 import workloads as W
-    srv = rq.Server(hbm_budget_bytes=48 * 3 * 50_000, query=rq.ANY, streams=3)  # 50k rays per worker
+    srv = rq.Server(hbm_budget_bytes=48 * 3 * 50_000, query=rq.ANY, streams=3)  # 50k rays per launch
     sid = srv.add_scene(scenes[0].scene)
     rays = _pinned((60_000, 8))
     rays[:] = _rays(W, scenes[0], 60_000, 9)
     hits = _pinned((60_000, 4))
-    with pytest.raises(rq.RQError) as e:
-        srv.submit(sid, rays, hits)  # larger than a worker arena
-    assert e.value.status == 8  # RQ_ERR_BUDGET
     with pytest.raises(rq.RQError) as e:
         srv.submit(99, rays[:10], hits[:10])
     assert e.value.status == 7  # RQ_ERR_NOT_FOUND
     with pytest.raises(rq.RQError) as e:
         srv.wait(123456)
     assert e.value.status == 7
-    # Queue more than the workers can hold; cancel the last queued one.
+    # Queue more than the pool can hold; cancel the last queued one.
     tickets = [srv.submit(sid, rays[:40_000], hits[:40_000]) for _ in range(8)]
     cancelled = srv.cancel(tickets[-1])
     for t in tickets[:-1]:
@@ -137,6 +134,42 @@ def test_failures_are_status_codes(rq, scenes):
             srv.wait(tickets[-1])
         assert e.value.status == 9  # RQ_ERR_CANCELLED
     srv.close()
+
+
+def test_budget_binds_and_large_requests_are_split(rq, scenes):
+    """A pool that holds about two launches: requests queue for bytes, the
+    bytes in use never exceed the budget, requests larger than one launch are
+    cut into pieces, and every result equals one plain trace of its rays."""
+    import torch
+    from cwbvh_b200 import workloads as W
+    per_launch = 30_000
+    budget = 2 * (per_launch * 48 + 512) + 256
+    srv = rq.Server(hbm_budget_bytes=budget, query=rq.ANY, streams=3, max_batch_rays=per_launch)
+    ids = [srv.add_scene(ds.scene) for ds in scenes]
+    rng = np.random.default_rng(5)
+    reqs = []
+    for k in range(14):
+        sid = k % len(scenes)
+        n = int(rng.integers(1000, 100_000)) if k % 3 else 95_001  # some span several launches
+        rays = _pinned((n, 8))
+        rays[:] = _rays(W, scenes[sid], n, 700 + k)
+        reqs.append((sid, rays, np.zeros((n, 4), np.float32) if k % 2 else _pinned((n, 4))))
+    tickets = [srv.submit(ids[sid], r, h) for sid, r, h in reqs]
+    stats = [srv.wait(t) for t in tickets]
+    mem = srv.memory()
+    srv.close()
+    assert all(s["status"] == 0 for s in stats)
+    assert mem["pool_bytes"] == budget // 256 * 256
+    assert 0 < mem["peak_in_use_bytes"] <= mem["pool_bytes"]
+    assert mem["admission_waits"] > 0  # the budget, not the streams, held requests back
+    assert mem["pieces"] == sum(-(-r.shape[0] // per_launch) for _, r, _ in reqs)
+    ctx = rq.Context()
+    for sid, rays, hits in reqs:
+        h = torch.empty((rays.shape[0], 4), device="cuda")
+        rq.trace(ctx, scenes[sid].scene, torch.from_numpy(rays).cuda(), h, rq.ANY)
+        ctx.check()
+        pi = scenes[sid].host.prim_index
+        assert np.array_equal(prim_ids(hits, pi) >= 0, prim_ids(h.cpu().numpy(), pi) >= 0)
 
 
 def _surfels(rq, ds, n, seed):
@@ -199,6 +232,34 @@ def test_bake_request_errors(rq, scenes):
     small = rq.Server(hbm_budget_bytes=48 * 3000, query=rq.ANY, streams=1)
     sid = small.add_scene(scenes[0].scene)
     big = np.zeros((200, 4), np.float32)
+    # one surfel's 4096 rays exceed a launch of this pool
     with pytest.raises(rq.RQError, match="BUDGET"):
-        small.submit_bake(sid, big, big, None, 32, 0, 0.0, 1.0, 0.0, np.zeros(200, np.float32))
+        small.submit_bake(sid, big, big, None, 4096, 0, 0.0, 1.0, 0.0, np.zeros(200, np.float32))
     small.close()
+
+
+def test_bake_request_split_into_pieces(rq, scenes):
+    """A bake request larger than one launch is cut into whole-surfel pieces
+    whose rays are generated with their indices in the whole request: the AO
+    equals rq_aorays + rq_trace + rq_ao_reduce over all of it."""
+    import torch
+    ds = scenes[1]
+    n, spp = 20_000, 16
+    pos, nrm, rad = _surfels(rq, ds, n, 77)
+    dg = ds.diag
+    args = (spp, 4321, 1e-4 * dg, 0.1 * dg, 0.5)
+    ctx = rq.Context()
+    rays = rq.aorays(torch.from_numpy(pos).cuda(), torch.from_numpy(nrm).cuda(), torch.from_numpy(rad).cuda(), spp,
+                     seed=args[1], tmin=args[2], tmax=args[3], offset_scale=args[4])
+    hits = torch.empty((rays.shape[0], 4), device="cuda")
+    rq.trace(ctx, ds.scene, rays, hits, rq.ANY)
+    ctx.check()
+    want = rq.ao_reduce(hits, n, spp).cpu().numpy()
+    srv = rq.Server(hbm_budget_bytes=8 << 20, query=rq.ANY, streams=2, max_batch_rays=50_000)
+    sid = srv.add_scene(ds.scene)
+    ao = _pinned((n,))
+    srv.wait(srv.submit_bake(sid, pos, nrm, rad, *args, ao))
+    mem = srv.memory()
+    srv.close()
+    assert mem["pieces"] > 1
+    assert np.array_equal(ao, want)
