@@ -1,9 +1,12 @@
 // Binned-SAH BVH builder.  It stands in for the reference's Embree build
 // (BuildBVH2Triangle / BuildBVH8Triangle, src/EmbreeBVHBuilder.cpp:303-478),
 // which is not available here.  A binary tree is built top-down with a binned
-// surface-area heuristic (object splits only; no spatial splits), then the
-// 8-wide tree for the CWBVH is made by collapsing it with a surface-area
-// cost model (see collapse_optimal).  Leaves of the 8-wide tree hold at most 3
+// surface-area heuristic: object splits, and binned spatial splits that
+// reference a triangle from both sides within a duplicate budget (200 % of the
+// triangle count by default), as Embree's high-quality builder does.  SAH
+// treelet restructuring then improves the binary tree, and the 8-wide tree for
+// the CWBVH is made by collapsing it with a surface-area cost model (see
+// collapse_optimal).  Leaves of the 8-wide tree hold at most 3
 // triangles, as the reference asks Embree for (maxLeafSize = 3,
 // src/EmbreeBVHBuilder.cpp:456-457).
 //

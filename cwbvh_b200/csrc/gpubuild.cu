@@ -416,9 +416,15 @@ __device__ inline int64_t key_tri(const uint64_t* k, int64_t pos, uint64_t idx_m
     return (int64_t)(k[pos] & idx_mask);
 }
 
+// Half the surface area of a box, and the SAH cost of a node over its two
+// children, with every rounding explicit: the treelet kernels (one thread or
+// one warp per treelet) compute the same costs bit for bit.
 __device__ inline float half_area(const float lo[3], const float hi[3]) {
-    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
-    return dx * dy + dy * dz + dz * dx;
+    const float dx = __fsub_rn(hi[0], lo[0]), dy = __fsub_rn(hi[1], lo[1]), dz = __fsub_rn(hi[2], lo[2]);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dy), __fmul_rn(dy, dz)), __fmul_rn(dz, dx));
+}
+__device__ inline float node_cost(float area, float c0, float c1) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(kCt, area), c0), c1);
 }
 
 __device__ inline void child_box(const BNode* nodes, const uint64_t* k, uint64_t idx_mask, const float* v,
@@ -432,7 +438,7 @@ __device__ inline void child_box(const BNode* nodes, const uint64_t* k, uint64_t
     } else {
         tri_box(v, idx, key_tri(k, ~code, idx_mask), lo, hi);
         count = 1;
-        if (cost) *cost = kCi * half_area(lo, hi);
+        if (cost) *cost = __fmul_rn(kCi, half_area(lo, hi));
     }
 }
 
@@ -460,7 +466,7 @@ __global__ void boxes_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, co
             nd.hi[a] = hi[a];
         }
         nd.count = c0 + c1;
-        nd.cost = kCt * half_area(lo, hi) + k0 + k1;
+        nd.cost = node_cost(half_area(lo, hi), k0, k1);
         node = nodes[node].parent;
     }
 }
@@ -540,10 +546,10 @@ __device__ void restructure(BNode* nodes, const uint64_t* k, uint64_t idx_mask, 
         // partitions {P, S \ P} with the lowest leaf in P, P != S
         for (int P = (S - 1) & S; P > 0; P = (P - 1) & S) {
             if (!(P & (1 << low))) continue;
-            const float c = cost[P] + cost[S ^ P];
+            const float c = __fadd_rn(cost[P], cost[S ^ P]);
             if (c < best) { best = c; bp = P; }
         }
-        cost[S] = kCt * half_area(slo, shi) + best;
+        cost[S] = __fadd_rn(__fmul_rn(kCt, half_area(slo, shi)), best);
         part[S] = (uint8_t)bp;
     }
     if (!(cost[full] < 0.999f * __ldcg(&nodes[root].cost))) return;
@@ -618,9 +624,275 @@ __global__ void treelet_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, 
         volatile BNode& nd = nodes[node];
         float lo[3], hi[3];
         for (int a = 0; a < 3; ++a) { lo[a] = fminf(l0[a], l1[a]); hi[a] = fmaxf(h0[a], h1[a]); }
-        nd.cost = kCt * half_area(lo, hi) + k0 + k1;
+        nd.cost = node_cost(half_area(lo, hi), k0, k1);
         if (c0 + c1 >= min_count) restructure(nodes, k, idx_mask, v, idx, leaf_parent, node);
         node = ld_parent(nodes, node);
+    }
+}
+
+// ---- The same restructuring with a warp per treelet (the parallel form of
+// Karras and Aila, section 4.2).  Lanes walk up the tree as in
+// treelet_kernel; at each step the nodes whose treelets are due are taken one
+// at a time by the whole warp: lane q holds leaf q while the treelet grows,
+// the subsets of one size are costed by different lanes (smaller subsets
+// first, so every partition's two parts are ready), and the 63 (31)
+// partitions of the 7-leaf (6-leaf) subsets are spread over the lanes and
+// reduced with shuffles.  Every subset's cost is the same expression in the
+// same order as in restructure(), and the chosen partition is the first
+// minimum in its enumeration order there, so the trees are identical.
+constexpr unsigned kWarpAll = 0xFFFFFFFFu;
+
+struct SubsetTable {
+    uint8_t set[127];   // the subsets of 7 leaves by size, then value
+    uint8_t start[9];   // first entry of each size (start[8] = 127)
+};
+constexpr SubsetTable make_subset_table() {
+    SubsetTable t{};
+    int k = 0;
+    for (int size = 1; size <= 7; ++size) {
+        t.start[size] = (uint8_t)k;
+        for (int S = 1; S < 128; ++S) {
+            int c = 0;
+            for (int b = 0; b < 7; ++b) c += (S >> b) & 1;
+            if (c == size) t.set[k++] = (uint8_t)S;
+        }
+    }
+    t.start[0] = 0;
+    t.start[8] = (uint8_t)k;
+    return t;
+}
+__constant__ SubsetTable c_subsets = make_subset_table();
+
+struct TreeletSmem {
+    float llo[kTreeletLeaves][3], lhi[kTreeletLeaves][3], lcost[kTreeletLeaves];
+    int32_t lcnt[kTreeletLeaves], leaf[kTreeletLeaves], inner[kTreeletLeaves - 1];
+    float cost[1 << kTreeletLeaves];
+    uint8_t part[1 << kTreeletLeaves];
+};
+
+// The i-th partition {P, S ^ P} of S in restructure()'s order: P holds the
+// lowest leaf of S, and P runs down from S - 1 over the subsets of S.
+__device__ inline int nth_partition(int S, int i) {
+    const int low = S & -S;
+    const int R = S ^ low;  // the other leaves
+    // Q = the i-th largest proper subset of R: the bits of (2^|R| - 2 - i)
+    // deposited into the positions of R.
+    const int nb = __popc(R);
+    int v = (1 << nb) - 2 - i, Q = 0, r = R;
+    for (int b = 0; b < nb; ++b) {
+        const int bit = r & -r;
+        if (v & (1 << b)) Q |= bit;
+        r ^= bit;
+    }
+    return low | Q;
+}
+
+__device__ void subset_box_s(const TreeletSmem& t, int n_leaf, int S, float lo[3], float hi[3]) {
+    for (int a = 0; a < 3; ++a) { lo[a] = FLT_MAX; hi[a] = -FLT_MAX; }
+    for (int q = 0; q < n_leaf; ++q)
+        if (S & (1 << q))
+            for (int a = 0; a < 3; ++a) { lo[a] = fminf(lo[a], t.llo[q][a]); hi[a] = fmaxf(hi[a], t.lhi[q][a]); }
+}
+
+// The whole warp restructures the treelet rooted at `root` (warp-uniform).
+__device__ void restructure_warp(BNode* nodes, const uint64_t* k, uint64_t idx_mask, const float* v,
+                                 const int32_t* idx, int32_t* leaf_parent, int32_t root, float root_cost,
+                                 TreeletSmem& t) {
+    const unsigned lane = threadIdx.x & 31u;
+    // Grow the treelet: lane q holds leaf q.
+    int32_t my_leaf = -1;
+    float mlo[3] = {0.f, 0.f, 0.f}, mhi[3] = {0.f, 0.f, 0.f}, mcost = 0.f, marea = -1.f;
+    int32_t mcnt = 0;
+    int n_in = 1, n_leaf = 2;
+    if (lane < 2) {
+        my_leaf = lane == 0 ? ld_left(nodes, root) : ld_right(nodes, root);
+        child_box(nodes, k, idx_mask, v, idx, my_leaf, mlo, mhi, mcnt, &mcost);
+        marea = half_area(mlo, mhi);
+    }
+    if (lane == 0) t.inner[0] = root;
+    while (n_leaf < kTreeletLeaves) {
+        // the first leaf of the largest area that is a node (restructure()'s scan)
+        float a = ((int)lane < n_leaf && my_leaf >= 0) ? marea : -1.f;
+        int best = ((int)lane < n_leaf && my_leaf >= 0) ? (int)lane : 64;
+        for (int o = 16; o > 0; o >>= 1) {
+            const float a2 = __shfl_xor_sync(kWarpAll, a, o);
+            const int b2 = __shfl_xor_sync(kWarpAll, best, o);
+            if (a2 > a || (a2 == a && b2 < best)) { a = a2; best = b2; }
+        }
+        if (best >= 64 || !(a > -1.f)) break;
+        const int32_t x = __shfl_sync(kWarpAll, my_leaf, best);
+        if (lane == 0) t.inner[n_in] = x;
+        ++n_in;
+        if ((int)lane == best || (int)lane == n_leaf) {
+            my_leaf = (int)lane == best ? ld_left(nodes, x) : ld_right(nodes, x);
+            child_box(nodes, k, idx_mask, v, idx, my_leaf, mlo, mhi, mcnt, &mcost);
+            marea = half_area(mlo, mhi);
+        }
+        ++n_leaf;
+    }
+    if (n_leaf < 3) return;
+    if ((int)lane < n_leaf) {
+        for (int a = 0; a < 3; ++a) { t.llo[lane][a] = mlo[a]; t.lhi[lane][a] = mhi[a]; }
+        t.lcost[lane] = mcost;
+        t.lcnt[lane] = mcnt;
+        t.leaf[lane] = my_leaf;
+        t.cost[1 << lane] = mcost;
+        t.part[1 << lane] = 0;
+    }
+    __syncwarp();
+    const int full = (1 << n_leaf) - 1;
+    for (int size = 2; size <= n_leaf; ++size) {
+        const int first = c_subsets.start[size], end = c_subsets.start[size + 1];
+        if (size < 6) {
+            // one subset per lane
+            for (int e = first + (int)lane; e < end; e += 32) {
+                const int S = c_subsets.set[e];
+                if (S > full) continue;
+                float slo[3], shi[3];
+                subset_box_s(t, n_leaf, S, slo, shi);
+                const int low = __ffs(S) - 1;
+                float bc = FLT_MAX;
+                int bp = 0;
+                for (int P = (S - 1) & S; P > 0; P = (P - 1) & S) {
+                    if (!(P & (1 << low))) continue;
+                    const float c = __fadd_rn(t.cost[P], t.cost[S ^ P]);
+                    if (c < bc) { bc = c; bp = P; }
+                }
+                t.cost[S] = __fadd_rn(__fmul_rn(kCt, half_area(slo, shi)), bc);
+                t.part[S] = (uint8_t)bp;
+            }
+        } else {
+            // one subset at a time, its partitions over the lanes
+            for (int e = first; e < end; ++e) {
+                const int S = c_subsets.set[e];
+                if (S > full) continue;
+                const int n_part = (1 << (__popc(S) - 1)) - 1;
+                float bc = FLT_MAX;
+                int bi = 1 << 30;
+                for (int i = (int)lane; i < n_part; i += 32) {
+                    const int P = nth_partition(S, i);
+                    const float c = __fadd_rn(t.cost[P], t.cost[S ^ P]);
+                    if (c < bc) { bc = c; bi = i; }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const float c2 = __shfl_xor_sync(kWarpAll, bc, o);
+                    const int i2 = __shfl_xor_sync(kWarpAll, bi, o);
+                    if (c2 < bc || (c2 == bc && i2 < bi)) { bc = c2; bi = i2; }
+                }
+                if (lane == 0) {
+                    float slo[3], shi[3];
+                    subset_box_s(t, n_leaf, S, slo, shi);
+                    t.cost[S] = __fadd_rn(__fmul_rn(kCt, half_area(slo, shi)), bc);
+                    t.part[S] = (uint8_t)(bi < n_part ? nth_partition(S, bi) : 0);
+                }
+                __syncwarp();
+            }
+        }
+        __syncwarp();
+    }
+    if (lane == 0 && t.cost[full] < 0.999f * root_cost) {
+        // every subset the new tree splits must have a split (finite costs);
+        // check before writing anything
+        bool ok = true;
+        {
+            int st[kTreeletLeaves], sp = 0;
+            st[sp++] = full;
+            while (sp > 0 && ok) {
+                const int S = st[--sp];
+                const int P = t.part[S];
+                if (P == 0 || (P & ~S) != 0 || P == S) { ok = false; break; }
+                if (P & (P - 1)) st[sp++] = P;
+                if ((S ^ P) & ((S ^ P) - 1)) st[sp++] = S ^ P;
+                if (sp > kTreeletLeaves - 1) ok = false;
+            }
+        }
+        if (ok) {
+            // rebuild top-down: subset -> node, internal nodes taken from `inner`
+            int32_t st_set[kTreeletLeaves], st_node[kTreeletLeaves];
+            int sp = 0, used = 1;
+            st_set[sp] = full;
+            st_node[sp++] = root;
+            while (sp > 0) {
+                --sp;
+                const int S = st_set[sp];
+                const int32_t nd = st_node[sp];
+                const int P = t.part[S];
+                const int side[2] = {P, S ^ P};
+                int32_t code[2];
+                for (int c = 0; c < 2; ++c) {
+                    const int T = side[c];
+                    if ((T & (T - 1)) == 0) {
+                        code[c] = t.leaf[__ffs(T) - 1];
+                        if (code[c] >= 0) nodes[code[c]].parent = nd;
+                        else leaf_parent[~code[c]] = nd;
+                    } else {
+                        const int32_t ni = t.inner[used++];
+                        code[c] = ni;
+                        nodes[ni].parent = nd;
+                        st_set[sp] = T;
+                        st_node[sp++] = ni;
+                    }
+                }
+                BNode& b = nodes[nd];
+                b.left = code[0];
+                b.right = code[1];
+                float slo[3], shi[3];
+                subset_box_s(t, n_leaf, S, slo, shi);
+                for (int a = 0; a < 3; ++a) { b.lo[a] = slo[a]; b.hi[a] = shi[a]; }
+                int32_t cnt = 0;
+                for (int q = 0; q < n_leaf; ++q)
+                    if (S & (1 << q)) cnt += t.lcnt[q];
+                b.count = cnt;
+                b.cost = t.cost[S];
+            }
+            __threadfence();
+        }
+    }
+    __syncwarp();
+}
+
+constexpr int kTreeletWarpBlock = 128;
+
+__global__ void __launch_bounds__(kTreeletWarpBlock) treelet_warp_kernel(
+        const uint64_t* k, uint64_t idx_mask, int64_t n, const float* v, const int32_t* idx, BNode* nodes,
+        int32_t* leaf_parent, int32_t* arrivals, int min_count) {
+    __shared__ TreeletSmem smem[kTreeletWarpBlock / 32];
+    TreeletSmem& t = smem[threadIdx.x / 32];
+    const unsigned lane = threadIdx.x & 31u;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t node = p < n ? leaf_parent[p] : -1;
+    for (;;) {
+        bool go = node >= 0;
+        if (go) {
+            __threadfence();
+            if (atomicAdd(&arrivals[node], 1) == 0) go = false;  // the sibling's thread finishes this node
+            __threadfence();
+        }
+        if (!go) node = -1;
+        float cost = 0.f;
+        bool due = false;
+        if (go) {
+            float l0[3], h0[3], l1[3], h1[3], k0, k1;
+            int32_t c0, c1;
+            child_box(nodes, k, idx_mask, v, idx, ld_left(nodes, node), l0, h0, c0, &k0);
+            child_box(nodes, k, idx_mask, v, idx, ld_right(nodes, node), l1, h1, c1, &k1);
+            volatile BNode& nd = nodes[node];
+            float lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) { lo[a] = fminf(l0[a], l1[a]); hi[a] = fmaxf(h0[a], h1[a]); }
+            cost = node_cost(half_area(lo, hi), k0, k1);
+            nd.cost = cost;
+            due = c0 + c1 >= min_count;
+        }
+        unsigned want = __ballot_sync(kWarpAll, due);
+        while (want) {
+            const int src = __ffs(want) - 1;
+            want &= want - 1;
+            const int32_t root = __shfl_sync(kWarpAll, node, src);
+            const float rc = __shfl_sync(kWarpAll, cost, src);
+            restructure_warp(nodes, k, idx_mask, v, idx, leaf_parent, root, rc, t);
+        }
+        if (go) node = ld_parent(nodes, node);
+        if (__ballot_sync(kWarpAll, node >= 0) == 0u) break;
     }
 }
 
@@ -1027,7 +1299,7 @@ __global__ void ploc_merge_kernel(const int32_t* nn, const int32_t* merge, const
         nd.lo[a] = u.lo[a];
         nd.hi[a] = u.hi[a];
     }
-    nd.cost = kCt * half_area(u.lo, u.hi) + cc[0] + cc[1];
+    nd.cost = node_cost(half_area(u.lo, u.hi), cc[0], cc[1]);
     for (int q = 0; q < 2; ++q) {
         if (c[q] >= 0) nodes[c[q]].parent = node;
         else leaf_parent[~c[q]] = node;
@@ -1200,6 +1472,8 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
                                         int method, int optimize_passes, int split_budget, rq_scene_t* out,
                                         void* stream) {
     if (!out || !vertices || !indices || nv <= 0 || nt <= 0 || nt > (int64_t)INT32_MAX / 4) return RQ_ERR_INVALID_ARG;
+    const bool thread_treelets = (method & RQ_GPU_BUILD_THREAD_TREELETS) != 0;
+    method &= ~RQ_GPU_BUILD_THREAD_TREELETS;
     if (method != RQ_GPU_BUILD_LBVH && method != RQ_GPU_BUILD_PLOC) return RQ_ERR_INVALID_ARG;
     if (split_budget < 0 || split_budget > 400) return RQ_ERR_INVALID_ARG;
     cudaStream_t s = (cudaStream_t)stream;
@@ -1297,8 +1571,12 @@ extern "C" rq_status rq_build_scene_gpu(const float* vertices, int64_t nv, const
         }
         for (int pass = 0; pass < optimize_passes && st == RQ_OK; ++pass) {
             ok(cudaMemsetAsync(arrivals, 0, (n - 1) * sizeof(int32_t), s), "rq_build_scene_gpu");
-            treelet_kernel<<<blocks_of(n, 128), 128, 0, s>>>(keys_sorted, idx_mask, n, bv, bi, bn,
-                                                             leaf_parent, arrivals, kTreeletLeaves);
+            if (thread_treelets)
+                treelet_kernel<<<blocks_of(n, 128), 128, 0, s>>>(keys_sorted, idx_mask, n, bv, bi, bn,
+                                                                 leaf_parent, arrivals, kTreeletLeaves);
+            else
+                treelet_warp_kernel<<<blocks_of(n, kTreeletWarpBlock), kTreeletWarpBlock, 0, s>>>(
+                    keys_sorted, idx_mask, n, bv, bi, bn, leaf_parent, arrivals, kTreeletLeaves);
             ok(cudaGetLastError(), "rq_build_scene_gpu");
         }
         if (st == RQ_OK) {

@@ -140,3 +140,19 @@ def test_duplicated_geometry(rq, po):
         ctx.check()
         want = po.trace(rq.CWBVH, nodes, woop, rays, False)
         assert np.array_equal(hits.cpu().numpy().view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("method,budget", [(0, 0), (1, 0), (1, 30)], ids=["lbvh", "ploc", "ploc-split30"])
+def test_warp_and_thread_treelets_give_the_same_tree(rq, method, budget):
+    """The treelet passes with a warp per treelet (the default) and with one
+    thread per treelet give byte-identical scenes."""
+    from cwbvh_b200 import workloads as W
+    V, I = W.scene_of_size(4, 200_000)
+    v, i = _device_mesh(V, I)
+    a = rq.Scene.build_gpu(v, i, optimize_passes=3, method=method, split_budget=budget).download()
+    b = rq.Scene.build_gpu(v, i, optimize_passes=3, method=method | rq.GPU_BUILD_THREAD_TREELETS,
+                           split_budget=budget).download()
+    none = rq.Scene.build_gpu(v, i, optimize_passes=0, method=method, split_budget=budget).download()
+    for x, y in zip(a, b):
+        assert x.shape == y.shape and np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    assert not np.array_equal(a[0].view(np.uint32)[:4096], none[0].view(np.uint32)[:4096])  # the passes did work
