@@ -35,6 +35,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "AO any-hit Mrays/s on 1 B200, batched/served vs plain launch; p50/p99 latency"
+BATCHED_WORKLOAD = "batched: 64 heightfield+box scenes, tris log-U[10k,2M], AO any-hit rays log-U[256K,8M]"
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 
 
@@ -237,6 +238,34 @@ def link_bound_ms(h2d_bytes: float, d2h_bytes: float, link: dict) -> float:
     return (small / each + (big - small) / rest_rate) * 1e3
 
 
+def issue_roofline(workload: str, rays_per_s: float, sm_mhz) -> dict:
+    """The bound the trace kernel actually meets: instruction issue.  Warp
+    instructions per ray come from the committed ncu capture of the same
+    kernel on a reduced case (profiles/issue_<workload>.json); the peak is one
+    warp instruction per scheduler per cycle: SMs x 4 x the median SM clock
+    sampled during the timed region."""
+    f = ROOT / "profiles" / f"issue_{workload}.json"
+    try:
+        prof = json.loads(f.read_text())
+    except Exception:
+        return None
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    except Exception:
+        sms = 148
+    if not sm_mhz:
+        return None
+    ipr = float(prof["warp_inst_per_ray"])
+    achieved = rays_per_s * ipr / 1e9
+    peak = sms * 4 * float(sm_mhz) * 1e6 / 1e9
+    return {"achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "G warp-inst/s",
+            "frac": round(achieved / peak, 4), "warp_inst_per_ray": ipr,
+            "thread_inst_per_warp_inst": prof.get("thread_inst_per_warp_inst"),
+            "peak_source": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz (median SM clock in the timed region)",
+            "source": prof.get("source")}
+
+
 def profile_traffic(workload: str):
     """DRAM bytes per launch of the trace kernel from the committed ncu summary, if any."""
     f = ROOT / "profiles" / f"traffic_{workload}.json"
@@ -302,6 +331,7 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving configuration")
+    ap.add_argument("--dump-reference-inputs", default="", help=argparse.SUPPRESS)
     ap.add_argument("--no-configs", action="store_true",
                     help="batched: skip the small, city and large configurations (run in their own processes)")
     ap.add_argument("--profile", action="store_true",
@@ -313,6 +343,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.dump_reference_inputs:
+        return dump_reference_inputs(args, args.dump_reference_inputs)
     if args.impl == "reference":
         return run_reference(args, world, rank, warmup)
 
@@ -561,8 +593,7 @@ def main():
         "dtype": "f32",
         "data": "synthetic (seeded procedural scenes and AO rays; the reference's mesh.dat/samplecache.dat are not shipped)",
         "config": {
-            "workload": ("batched: 64 heightfield+box scenes, tris log-U[10k,2M], AO any-hit rays log-U[256K,8M], "
-                         "one persistent launch, " +
+            "workload": (BATCHED_WORKLOAD + ", one persistent launch, " +
                          ("Morton sort (threshold %d rays), " % bp.sort_threshold if bp.sort_threshold >= 0
                           else "Morton sort off (autotuner), ") +
                          ("CUDA graph, " if bp.use_graph else "") + "autotuned")
@@ -607,7 +638,9 @@ def main():
                             "peak_source": "rq_probe_l2_read_shape: best of 24 shapes (8-48 MB L2-resident buffers, "
                                            "coalesced 16 B L1-bypassing loads, SMs x 8/16/32 blocks, 4/8 loads in "
                                            "flight), measured in this run",
-                            "best_shape": l2["best"]}},
+                            "best_shape": l2["best"]},
+                     "issue": issue_roofline(args.workload + ("_quick" if args.quick else ""),
+                                             total_rays / (ms_kernel * 1e-3), clocks.get("sm_mhz"))},
         "gpu_launches": int(launches_per_step * args.steps),
         "clocks": clocks,
         "clocks_ms_per_step": round(ms_batch2, 4),
@@ -1343,17 +1376,47 @@ def run_large(args, world, rank, dist):
         print(json.dumps(line), flush=True)
 
 
+def dump_reference_inputs(args, path: str) -> None:
+    """Writes the reference arm's inputs -- each scene's CWBVH node and Woop
+    buffers and the bounded ray sample -- to an .npz, so that the arm's own
+    process times the CPU traversal without loading librq."""
+    spec = workload_spec(args.workload, args.quick, 0)
+    built = build_scenes(spec)
+    sample = cpu_sample(spec, built, target_rays=1 << 20)
+    arrays = {}
+    for k, (hb, rays) in enumerate(sample):
+        arrays[f"nodes{k}"] = np.ascontiguousarray(hb.nodes)
+        arrays[f"woop{k}"] = np.ascontiguousarray(hb.woop)
+        arrays[f"rays{k}"] = rays
+    np.savez(path, n=len(sample), triangles=sum(s["tris"] for s in spec),
+             rays_total=sum(s["rays"] for s in spec), **arrays)
+
+
 def run_reference(args, world, rank, warmup):
     """Reference arm: the reference has no CPU traversal, so its path is timed
     through the C restatement (oracle/oracle.c, kind "port") on the host cores,
-    each step a bounded sample of the same workload."""
+    each step a bounded sample of the same workload.  The scenes are built and
+    the sample drawn by a child process (which loads librq); this process only
+    loads the restatement."""
     if rank != 0:
         return
-    spec = workload_spec(args.workload, args.quick, 0)
-    built = build_scenes(spec)
+    import tempfile
+    import types
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "ref_inputs.npz")
+        cmd = [sys.executable, str(ROOT / "bench.py"), "--workload", args.workload, "--dump-reference-inputs", path]
+        if args.quick:
+            cmd.append("--quick")
+        env = dict(os.environ)
+        for k in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "LOCAL_WORLD_SIZE"):
+            env.pop(k, None)
+        subprocess.run(cmd, check=True, env=env, cwd=str(ROOT))
+        z = np.load(path)
+        sample = [(types.SimpleNamespace(nodes=z[f"nodes{k}"], woop=z[f"woop{k}"]), z[f"rays{k}"])
+                  for k in range(int(z["n"]))]
+        tris, rays_total = int(z["triangles"]), int(z["rays_total"])
     from oracle import pyoracle as po
     threads = po.oracle().oracle_max_threads()
-    sample = cpu_sample(spec, built, target_rays=1 << 20)
     for _ in range(min(warmup, 1)):
         time_cpu(sample, threads)
     dt, n = 0.0, 0
@@ -1362,11 +1425,15 @@ def run_reference(args, world, rank, warmup):
         dt += d
         n += k
     value = n / dt / 1e6
+    workload = BATCHED_WORKLOAD if args.workload == "batched" and not args.quick else \
+        f"{args.workload}{' (quick)' if args.quick else ''}"
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps,
         "warmup": warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batched (bounded sample per step)" if args.workload == "batched" else args.workload},
+        "config": {"workload": workload, "triangles": tris, "rays_per_gpu": rays_total, "query": "any-hit",
+                   "sample_per_step": f"{n // args.steps} rays drawn from all scenes in proportion to their ray "
+                                      "counts (a bounded sample of the workload)"},
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads, "kind": "port",
                          "sample": f"{n // args.steps} rays per step from all scenes; the reference has no CPU "
