@@ -332,6 +332,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiler runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving configuration")
     ap.add_argument("--dump-reference-inputs", default="", help=argparse.SUPPRESS)
+    ap.add_argument("--subset", type=int, default=0,
+                    help="batched: only the first N scenes (reduced cases for profiler captures)")
+    ap.add_argument("--ray-cap", type=int, default=0, help="batched: at most this many rays per scene")
     ap.add_argument("--no-configs", action="store_true",
                     help="batched: skip the small, city and large configurations (run in their own processes)")
     ap.add_argument("--profile", action="store_true",
@@ -369,6 +372,11 @@ def main():
         return
 
     spec = workload_spec(args.workload, args.quick, rank)
+    if args.subset > 0:
+        spec = spec[:args.subset]
+    if args.ray_cap > 0:
+        for sp in spec:
+            sp["rays"] = min(sp["rays"], args.ray_cap)
     t0 = time.time()
     built = build_scenes(spec)
     log(f"[bench] built {len(spec)} scenes, {sum(s['tris'] for s in spec)/1e6:.1f}M tris in {time.time()-t0:.1f}s")

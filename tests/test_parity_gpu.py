@@ -13,7 +13,7 @@ from adjudicate import compare
 
 pytestmark = pytest.mark.gpu
 
-N_RAYS = 200_000
+N_RAYS = 1 << 20  # config 0's ray count
 
 
 @pytest.fixture(scope="module")
@@ -46,6 +46,33 @@ def test_ordered_bit_exact(rq, po, small, kind, query):
     want = po.trace(kind, ds.host.nodes, ds.host.woop, r, query == rq.ANY)
     res = compare(po, r, got, want, ds.host.prim_index, V, I, query == rq.ANY, exact=True)
     assert res["hits"] > N_RAYS // 10
+
+
+@pytest.mark.parametrize("query", [0, 1], ids=["closest", "any"])
+def test_slab_extreme_paths_bit_exact(rq, po, small, query):
+    """A ray with tmin > 0 in a scene of moderate coordinates takes the
+    three-input float slab extremes, any other ray the reference's
+    integer-ordered ones; both decide every child alike.  Rays of both kinds
+    mixed in every warp, and a scene whose coordinates exceed 2^46 (where
+    only the integer form is used), equal the oracle bit for bit."""
+    from cwbvh_b200 import workloads as W
+    V, I, scenes, rays = small
+    r = rays[:200_000].cpu().numpy().copy()
+    r[::3, 3] = 0.0  # tmin = 0 on every third ray
+    r[1::7, 3] = -1.0  # and negative on some
+    import torch
+    ctx = rq.Context()
+    cases = [(scenes[rq.CWBVH], V, r)]
+    Vb = (V.astype(np.float64) * 1e15).astype(np.float32)
+    big = W.upload(Vb, I, rq.CWBVH)
+    rb = W.ao_rays(big, 200_000, seed=77).cpu().numpy()
+    rb[::4, 3] = 0.0
+    cases.append((big, Vb, rb))
+    for ds, VV, rr in cases:
+        got = _run(rq, rq.trace_ordered, ctx, ds, torch.from_numpy(rr).cuda(), query)
+        want = po.trace(rq.CWBVH, ds.host.nodes, ds.host.woop, rr, query == rq.ANY)
+        res = compare(po, rr, got, want, ds.host.prim_index, VV, I, query == rq.ANY, exact=True)
+        assert res["hits"] > 0
 
 
 @pytest.mark.parametrize("kind", [0, 1], ids=["cwbvh", "bvh2"])
