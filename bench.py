@@ -254,15 +254,20 @@ def issue_roofline(workload: str, rays_per_s: float, sm_mhz) -> dict:
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     except Exception:
         sms = 148
+    clock_note = "median SM clock in the timed region"
     if not sm_mhz:
-        return None
+        try:
+            sm_mhz = float(json.loads(PEAKS.read_text())["sm_max_mhz"])
+            clock_note = "sm_max_mhz of MEASURED_PEAKS.json (clocks not sampled in this run)"
+        except Exception:
+            return None
     ipr = float(prof["warp_inst_per_ray"])
     achieved = rays_per_s * ipr / 1e9
     peak = sms * 4 * float(sm_mhz) * 1e6 / 1e9
     return {"achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "G warp-inst/s",
             "frac": round(achieved / peak, 4), "warp_inst_per_ray": ipr,
             "thread_inst_per_warp_inst": prof.get("thread_inst_per_warp_inst"),
-            "peak_source": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz (median SM clock in the timed region)",
+            "peak_source": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz ({clock_note})",
             "source": prof.get("source")}
 
 
@@ -1375,6 +1380,7 @@ def run_large(args, world, rank, dist):
                      "traffic": (profile_traffic("large" + ("_quick" if args.quick else "")) or {}).get(
                          "dram_bytes_per_launch"),
                      "l2": {"peak": round(l2, 1), "frac": unsorted["l2_frac"]},
+                     "issue": issue_roofline("large" + ("_quick" if args.quick else ""), n / (ms_plain * 1e-3), None),
                      "kernel": "unsorted AO any-hit trace"},
     }
     line = _single_line(args, world, warmup, f"large: {I.shape[0]/1e6:.1f}M tris, {n_surf} surfels x {spp} spp "

@@ -75,12 +75,22 @@ __device__ __forceinline__ bool woop_test(const float4& v0, const float4& v1, co
     return (t > tmin && t < tmax) && (u >= 0.0f && u <= 1.0f) && (v >= 0.0f && __fadd_rn(u, v) <= 1.0f);
 }
 
-// Exact float of byte `byte_index` of a word (every byte value is a float).
-// Written as the integer conversion of the extracted byte: on sm_100a this
-// measured 14 % fewer warp instructions per ray for the whole trace kernel
-// than building 2^23 + b with a byte permute and subtracting 2^23.
+// Exact float of byte `byte_index` of a word (every byte value is a float),
+// two ways that run on different pipes.  The integer conversion of the
+// extracted byte takes fewer instructions (the whole trace kernel issues 14 %
+// fewer warp instructions per ray than with the permute form alone) but runs
+// on the XU pipe; building 2^23 + b with a byte permute and subtracting 2^23
+// runs on the ALU and FMA pipes.  The slab test converts the x and y bytes
+// the first way and the z bytes the second, which measured 1-3 % faster than
+// either way alone.
 __device__ __forceinline__ float byte_to_float(unsigned word, unsigned byte_index) {
     return __uint2float_rn((word >> (8u * byte_index)) & 0xFFu);
+}
+__device__ __forceinline__ float byte_to_float_permute(unsigned word, unsigned byte_index) {
+    const unsigned sel = 0x7540u | byte_index;  // bytes: [word.b<i>, 0, 0, 0x4B]
+    unsigned r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(word), "r"(0x4B000000u), "r"(sel));
+    return __fsub_rn(__uint_as_float(r), 8388608.0f);
 }
 
 // Hit mask of the 8 children of one CWBVH node (src/TraversalKernelCWBVH.cu:
@@ -112,10 +122,10 @@ __device__ __forceinline__ unsigned cwbvh_hitmask(const float4& n1, const float4
         for (int c = 0; c < 4; ++c) {
             const float tx0 = __fmaf_rn(byte_to_float(lox, c), adjx, orx);
             const float ty0 = __fmaf_rn(byte_to_float(loy, c), adjy, ory);
-            const float tz0 = __fmaf_rn(byte_to_float(loz, c), adjz, orz);
+            const float tz0 = __fmaf_rn(byte_to_float_permute(loz, c), adjz, orz);
             const float tx1 = __fmaf_rn(byte_to_float(hix, c), adjx, orx);
             const float ty1 = __fmaf_rn(byte_to_float(hiy, c), adjy, ory);
-            const float tz1 = __fmaf_rn(byte_to_float(hiz, c), adjz, orz);
+            const float tz1 = __fmaf_rn(byte_to_float_permute(hiz, c), adjz, orz);
             const float cmin = fmaxf(imax3(tx0, ty0, tz0), tmin);
             const float cmax = fminf(imin3(tx1, ty1, tz1), tmax);
             if (cmin <= cmax) hitmask |= ((bits4 >> (8 * c)) & 0xFFu) << ((bitidx4 >> (8 * c)) & 0xFFu);
