@@ -894,13 +894,53 @@ def run_ref_gpu(scenes, rays, warmup: int, steps: int, kind: int = 0):
     per_call = [float(m) for m in re.findall(r"([0-9.]+)MS, [0-9.]+MRays/s \(" + tag, txt)]
     timed = per_call[len(per_call) - steps * len(rays):] if len(per_call) >= steps * len(rays) else []
     ms = sum(timed) / steps if timed else wall_ms
+    out = {"value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
+           "wall_ms_per_step": round(wall_ms, 3),
+           "query": "closest-hit (the reference has no any-hit kernel)",
+           "timing": f"sum of the reference's own CUDA-event kernel times (its log line per {tag} call)"
+           if timed else f"host wall clock around synchronous {tag} calls",
+           "grid": "as shipped (CWBVH: 32x32 blocks of 32x2 threads; BVH2: one 128-thread block per 128 rays)"}
+    if kind == 0:
+        out["occupancy_filling_grid"] = ref_cwbvh_full_grid(lib, scenes, rays, warmup, steps, total)
+    return out, [h for h in out_hits]
+
+
+def ref_cwbvh_full_grid(lib, scenes, rays, warmup: int, steps: int, total: int) -> dict:
+    """The reference's own CWBVH kernel, unmodified, launched with as many
+    32x2-thread blocks as are resident at once on the device instead of its
+    shipped 32x32 grid (oracle/ref_harness.cu, ref_trace_cwbvh_grid), timed
+    with CUDA events on the legacy default stream it runs on: what the
+    reference's kernel does on a grid that fills a B200."""
+    import ctypes as C
+    import torch
+    counter = torch.zeros(1, dtype=torch.int32, device="cuda")
+    hits = [torch.empty((r.shape[0], 4), device="cuda") for r in rays]
+    used = C.c_int(0)
+
+    def step():
+        for ds, r, h in zip(scenes, rays, hits):
+            dn, dw, dp = C_buffers(ds.scene)
+            lib.ref_bind_cwbvh(dn, dw, dp)
+            err = lib.ref_trace_cwbvh_grid(r.data_ptr(), h.data_ptr(), r.shape[0], 0, counter.data_ptr(),
+                                           C.byref(used))
+            if err:
+                raise RuntimeError(f"ref_trace_cwbvh_grid: CUDA error {err}")
+    stream = torch.cuda.default_stream()
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
     return {"value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms_per_step": round(ms, 3),
-            "wall_ms_per_step": round(wall_ms, 3),
-            "query": "closest-hit (the reference has no any-hit kernel)",
-            "timing": f"sum of the reference's own CUDA-event kernel times (its log line per {tag} call)"
-            if timed else f"host wall clock around synchronous {tag} calls",
-            "grid": "as shipped (CWBVH: 32x32 blocks of 32x2 threads; BVH2: one 128-thread block per 128 rays)"
-            }, [h for h in out_hits]
+            "blocks": int(used.value), "grid": f"{used.value} blocks of 32x2 threads ({used.value / sms:.0f} per SM, "
+                                              "all resident at once); shipped: 1024 blocks",
+            "timing": "CUDA events around the launches (scene binds included)"}
 
 
 def C_buffers(scene):

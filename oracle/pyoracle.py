@@ -66,6 +66,8 @@ def ref():
         lib.ref_aorays.restype = vp
         lib.ref_aorays.argtypes = [C.c_int, C.c_int, vp, vp, vp]
         lib.ref_cuda_free.argtypes = [vp]
+        lib.ref_trace_cwbvh_grid.restype = C.c_int
+        lib.ref_trace_cwbvh_grid.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.POINTER(C.c_int)]
         lib.ref_sync.restype = C.c_int
         _ref = lib
     return _ref

@@ -4,7 +4,8 @@
 //   * ConvertToGPUBVH2 / ConvertToGPUCompressedWideBVH / WoopifyTriangle
 //     (src/GPUBVHConverter.cpp:10-403), fed with this library's builder trees;
 //   * rtBind*/rtTrace* (src/TraversalKernelCWBVH.cu:377-426,
-//     src/TraversalKernelBVH2.cu:180-227), the reference's CUDA kernels;
+//     src/TraversalKernelBVH2.cu:180-227), the reference's CUDA kernels, and
+//     the CWBVH kernel launched with an occupancy-filling grid;
 //   * GenerateAORaysUniform (src/ValidationKernels.cu:140-187).
 // No reference source is copied here; they are compiled where they lie.
 #include <cstdint>
@@ -18,6 +19,10 @@
 #include "TraversalKernelBVH2.h"
 #include "TraversalKernelCWBVH.h"
 #include "ValidationKernels.h"
+
+// The reference's persistent CWBVH kernel (defined in
+// src/TraversalKernelCWBVH.cu, compiled in its own object).
+__global__ void rtTraceCWBVHDynamicFetch(Ray* rayBuffer, Hit* rayResultBuffer, int rayCount, int* finishedRayCount);
 
 namespace {
 
@@ -128,6 +133,31 @@ void ref_bind_bvh2(const void* nodes, const void* woop, const int32_t* prim) {
     rtBindBVH2Data((const float4*)nodes, (const float4*)woop, prim);
 }
 void ref_trace_bvh2(void* rays, void* hits, int n) { rtTraceBVH2((Ray*)rays, (Hit*)hits, n); }
+
+// The reference's CWBVH kernel itself (src/TraversalKernelCWBVH.cu:24-29: its
+// blocks are 32 x 2 threads, its grid persistent with a global ray counter),
+// launched with `blocks` blocks instead of rtTraceCWBVH's fixed 32 x 32
+// (src/TraversalKernelCWBVH.cu:401-402), on the legacy default stream like
+// rtTraceCWBVH.  blocks <= 0: as many as are resident at once on the device
+// (occupancy-filling).  `counter` is a device int the call zeroes first.
+// Returns the CUDA error code of the launch (the caller waits for it);
+// *used_blocks receives the grid size.
+int ref_trace_cwbvh_grid(void* rays, void* hits, int n, int blocks, int* counter, int* used_blocks) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rtTraceCWBVHDynamicFetch, 64, 0);
+    if (e != cudaSuccess) return (int)e;
+    if (blocks <= 0) blocks = sms * (per_sm > 0 ? per_sm : 1);
+    if (used_blocks) *used_blocks = blocks;
+    e = cudaMemsetAsync(counter, 0, sizeof(int), 0);
+    if (e == cudaSuccess) {
+        rtTraceCWBVHDynamicFetch<<<blocks, dim3(32, 2)>>>((Ray*)rays, (Hit*)hits, n, counter);
+        e = cudaGetLastError();
+    }
+    return (int)e;
+}
 
 // Reference AO ray generation (curand XORWOW); returns a device buffer owned
 // by the caller (cudaFree).

@@ -95,3 +95,32 @@ def test_dropin_adapters(rq, po, setup, kind):
     occl(rays, hits, rays.shape[0])
     wa = po.trace(kind, hb.nodes, hb.woop, r, True)
     assert np.array_equal(prim_ids(hits.cpu().numpy(), hb.prim_index) >= 0, prim_ids(wa, hb.prim_index) >= 0)
+
+
+def test_reference_kernel_on_an_occupancy_filling_grid(rq, po, setup):
+    """The reference's CWBVH kernel, unmodified, on as many resident 32x2
+    blocks as the device holds (the bench's second reference figure): the
+    rays it writes agree with the oracle up to adjudicated ties, as on its
+    shipped 32x32 grid."""
+    import torch
+    if not po.ref_available():
+        pytest.skip("oracle/_ref not built")
+    V, I, scenes, rays = setup
+    ds = scenes[rq.CWBVH]
+    lib = po.ref()
+    n, w, p = _buffers(rq, ds.scene)
+    lib.ref_bind_cwbvh(n, w, p)
+    hits = torch.full((rays.shape[0], 4), float("nan"), device="cuda")
+    counter = torch.zeros(1, dtype=torch.int32, device="cuda")
+    used = C.c_int(0)
+    assert lib.ref_trace_cwbvh_grid(rays.data_ptr(), hits.data_ptr(), rays.shape[0], 0, counter.data_ptr(),
+                                    C.byref(used)) == 0
+    assert lib.ref_sync() == 0
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    assert used.value > 1024 and used.value % sms == 0  # more than the shipped 32x32 grid
+    ref = hits.cpu().numpy()
+    written = ~np.isnan(ref[:, 0])
+    assert int((~written).sum()) <= rays.shape[0] // 50
+    r = rays.cpu().numpy()
+    want = po.trace(rq.CWBVH, ds.host.nodes, ds.host.woop, r[written], False)
+    compare(po, r[written], ref[written], want, ds.host.prim_index, V, I, any_hit=False)
