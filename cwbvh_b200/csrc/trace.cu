@@ -175,41 +175,57 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
         int lost = 0;
         for (;;) {
             // ---- node phase: take the nearest child of the current node group
+            auto node_step = [&]() -> unsigned {
+                unsigned fault = 0u;
+                const unsigned hitsm = ng.y;
+                const unsigned bit = highest_bit(hitsm);
+                const unsigned base = ng.x;
+                ng.y &= ~(1u << bit);
+                if (ng.y > 0x00FFFFFFu && !push(ng)) fault = kErrStackOverflow;
+                const unsigned slot = (bit - 24u) ^ octinv;
+                const unsigned ci = base + (unsigned)__popc(hitsm & ~(0xFFFFFFFFu << slot));
+                if (++steps > p.step_limit) fault |= kErrTimeout;
+                if ((uint64_t)ci * 5u + 5u > (uint64_t)L.node_f4) fault |= kErrBadScene;
+                if (!fault) {
+                    const float4* np = L.nodes + (size_t)ci * 5u;
+                    const float4 n0 = ld_nc(np + 0), n1 = ld_nc(np + 1), n2 = ld_nc(np + 2);
+                    const float4 n3 = ld_nc(np + 3), n4 = ld_nc(np + 4);
+                    if (COUNT) ++nvis;
+                    const unsigned ew = __float_as_uint(n0.w);
+                    const float adjx = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)(ew & 0xFFu) + 127)) << 23), idx_);
+                    const float adjy = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)((ew >> 8) & 0xFFu) + 127)) << 23), idy);
+                    const float adjz = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)((ew >> 16) & 0xFFu) + 127)) << 23), idz);
+                    const float orx = __fmul_rn(-__fsub_rn(ox, n0.x), idx_);
+                    const float ory = __fmul_rn(-__fsub_rn(oy, n0.y), idy);
+                    const float orz = __fmul_rn(-__fsub_rn(oz, n0.z), idz);
+                    const bool negx = idx_ < 0.f, negy = idy < 0.f, negz = idz < 0.f;
+                    const unsigned hitmask = cwbvh_hitmask(n1, n2, n3, n4, adjx, adjy, adjz, orx, ory, orz, negx,
+                                                           negy, negz, octinv4, tmin, tmax);
+                    ng = make_uint2(__float_as_uint(n1.x), (hitmask & 0xFF000000u) | (ew >> 24));
+                    tg = make_uint2(__float_as_uint(n1.y), hitmask & 0x00FFFFFFu);
+                }
+                return fault;
+            };
             unsigned fault = 0u;
             if (active) {
                 if (ng.y > 0x00FFFFFFu) {
-                    const unsigned hitsm = ng.y;
-                    const unsigned bit = highest_bit(hitsm);
-                    const unsigned base = ng.x;
-                    ng.y &= ~(1u << bit);
-                    if (ng.y > 0x00FFFFFFu && !push(ng)) fault = kErrStackOverflow;
-                    const unsigned slot = (bit - 24u) ^ octinv;
-                    const unsigned ci = base + (unsigned)__popc(hitsm & ~(0xFFFFFFFFu << slot));
-                    if (++steps > p.step_limit) fault |= kErrTimeout;
-                    if ((uint64_t)ci * 5u + 5u > (uint64_t)L.node_f4) fault |= kErrBadScene;
-                    if (!fault) {
-                        const float4* np = L.nodes + (size_t)ci * 5u;
-                        const float4 n0 = ld_nc(np + 0), n1 = ld_nc(np + 1), n2 = ld_nc(np + 2);
-                        const float4 n3 = ld_nc(np + 3), n4 = ld_nc(np + 4);
-                        if (COUNT) ++nvis;
-                        const unsigned ew = __float_as_uint(n0.w);
-                        const float adjx = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)(ew & 0xFFu) + 127)) << 23), idx_);
-                        const float adjy = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)((ew >> 8) & 0xFFu) + 127)) << 23), idy);
-                        const float adjz = __fmul_rn(__uint_as_float(((unsigned)((int)(signed char)((ew >> 16) & 0xFFu) + 127)) << 23), idz);
-                        const float orx = __fmul_rn(-__fsub_rn(ox, n0.x), idx_);
-                        const float ory = __fmul_rn(-__fsub_rn(oy, n0.y), idy);
-                        const float orz = __fmul_rn(-__fsub_rn(oz, n0.z), idz);
-                        const bool negx = idx_ < 0.f, negy = idy < 0.f, negz = idz < 0.f;
-                        const unsigned hitmask = cwbvh_hitmask(n1, n2, n3, n4, adjx, adjy, adjz, orx, ory, orz, negx,
-                                                               negy, negz, octinv4, tmin, tmax);
-                        ng = make_uint2(__float_as_uint(n1.x), (hitmask & 0xFF000000u) | (ew >> 24));
-                        tg = make_uint2(__float_as_uint(n1.y), hitmask & 0x00FFFFFFu);
-                    }
+                    fault = node_step();
                 } else {
                     tg = ng;
                     ng = make_uint2(0u, 0u);
                 }
                 if (fault) finish(fault);
+            }
+            // Any-hit: a lane whose node produced no triangles and has inner
+            // children left descends once more in the same iteration, in the
+            // order the next iteration would take (+2 % batched any-hit;
+            // closest-hit loses 6-10 %: its triangle tests, which shrink
+            // tmax, get postponed more often).
+            if (ANY && __ballot_sync(kFullMask, active && tg.y == 0u && ng.y > 0x00FFFFFFu)) {
+                if (active && tg.y == 0u && ng.y > 0x00FFFFFFu) {
+                    const unsigned f2 = node_step();
+                    if (f2) finish(f2);
+                }
             }
 
             // ---- triangle phase, warp-synchronous; postpone when few lanes remain
