@@ -635,10 +635,11 @@ __global__ void treelet_kernel(const uint64_t* k, uint64_t idx_mask, int64_t n, 
 // treelet_kernel; at each step the nodes whose treelets are due are taken one
 // at a time by the whole warp: lane q holds leaf q while the treelet grows,
 // the subsets of one size are costed by different lanes (smaller subsets
-// first, so every partition's two parts are ready), and the 63 (31)
-// partitions of the 7-leaf (6-leaf) subsets are spread over the lanes and
-// reduced with shuffles.  Every subset's cost is the same expression in the
-// same order as in restructure(), and the chosen partition is the first
+// first, so every partition's two parts are ready; a subset's box is its
+// box without its highest leaf, kept in shared memory, joined with that
+// leaf's), and the 63 partitions of the 7-leaf set are spread over the lanes
+// and reduced with shuffles.  Every subset's cost is the same expression in
+// the same order as in restructure(), and the chosen partition is the first
 // minimum in its enumeration order there, so the trees are identical.
 constexpr unsigned kWarpAll = 0xFFFFFFFFu;
 
@@ -667,6 +668,7 @@ struct TreeletSmem {
     float llo[kTreeletLeaves][3], lhi[kTreeletLeaves][3], lcost[kTreeletLeaves];
     int32_t lcnt[kTreeletLeaves], leaf[kTreeletLeaves], inner[kTreeletLeaves - 1];
     float cost[1 << kTreeletLeaves];
+    float slo[1 << kTreeletLeaves][3], shi[1 << kTreeletLeaves][3];  // subset boxes
     uint8_t part[1 << kTreeletLeaves];
 };
 
@@ -687,11 +689,18 @@ __device__ inline int nth_partition(int S, int i) {
     return low | Q;
 }
 
-__device__ void subset_box_s(const TreeletSmem& t, int n_leaf, int S, float lo[3], float hi[3]) {
-    for (int a = 0; a < 3; ++a) { lo[a] = FLT_MAX; hi[a] = -FLT_MAX; }
-    for (int q = 0; q < n_leaf; ++q)
-        if (S & (1 << q))
-            for (int a = 0; a < 3; ++a) { lo[a] = fminf(lo[a], t.llo[q][a]); hi[a] = fmaxf(hi[a], t.lhi[q][a]); }
+// The box of subset S (two or more leaves) from the box of S without its
+// highest leaf, already in the table, and that leaf's box; min / max are
+// exact in any order, so it equals restructure()'s box of the same leaves.
+__device__ void subset_box_s(TreeletSmem& t, int S, float lo[3], float hi[3]) {
+    const int high = 31 - __clz(S);
+    const int R = S & ~(1 << high);
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = fminf(t.slo[R][a], t.llo[high][a]);
+        hi[a] = fmaxf(t.shi[R][a], t.lhi[high][a]);
+        t.slo[S][a] = lo[a];
+        t.shi[S][a] = hi[a];
+    }
 }
 
 // The whole warp restructures the treelet rooted at `root` (warp-uniform).
@@ -732,7 +741,12 @@ __device__ void restructure_warp(BNode* nodes, const uint64_t* k, uint64_t idx_m
     }
     if (n_leaf < 3) return;
     if ((int)lane < n_leaf) {
-        for (int a = 0; a < 3; ++a) { t.llo[lane][a] = mlo[a]; t.lhi[lane][a] = mhi[a]; }
+        for (int a = 0; a < 3; ++a) {
+            t.llo[lane][a] = mlo[a];
+            t.lhi[lane][a] = mhi[a];
+            t.slo[1 << lane][a] = mlo[a];
+            t.shi[1 << lane][a] = mhi[a];
+        }
         t.lcost[lane] = mcost;
         t.lcnt[lane] = mcnt;
         t.leaf[lane] = my_leaf;
@@ -743,13 +757,13 @@ __device__ void restructure_warp(BNode* nodes, const uint64_t* k, uint64_t idx_m
     const int full = (1 << n_leaf) - 1;
     for (int size = 2; size <= n_leaf; ++size) {
         const int first = c_subsets.start[size], end = c_subsets.start[size + 1];
-        if (size < 6) {
+        if (size < 7) {
             // one subset per lane
             for (int e = first + (int)lane; e < end; e += 32) {
                 const int S = c_subsets.set[e];
                 if (S > full) continue;
                 float slo[3], shi[3];
-                subset_box_s(t, n_leaf, S, slo, shi);
+                subset_box_s(t, S, slo, shi);
                 const int low = __ffs(S) - 1;
                 float bc = FLT_MAX;
                 int bp = 0;
@@ -781,7 +795,7 @@ __device__ void restructure_warp(BNode* nodes, const uint64_t* k, uint64_t idx_m
                 }
                 if (lane == 0) {
                     float slo[3], shi[3];
-                    subset_box_s(t, n_leaf, S, slo, shi);
+                    subset_box_s(t, S, slo, shi);
                     t.cost[S] = __fadd_rn(__fmul_rn(kCt, half_area(slo, shi)), bc);
                     t.part[S] = (uint8_t)(bi < n_part ? nth_partition(S, bi) : 0);
                 }
@@ -836,9 +850,7 @@ __device__ void restructure_warp(BNode* nodes, const uint64_t* k, uint64_t idx_m
                 BNode& b = nodes[nd];
                 b.left = code[0];
                 b.right = code[1];
-                float slo[3], shi[3];
-                subset_box_s(t, n_leaf, S, slo, shi);
-                for (int a = 0; a < 3; ++a) { b.lo[a] = slo[a]; b.hi[a] = shi[a]; }
+                for (int a = 0; a < 3; ++a) { b.lo[a] = t.slo[S][a]; b.hi[a] = t.shi[S][a]; }
                 int32_t cnt = 0;
                 for (int q = 0; q < n_leaf; ++q)
                     if (S & (1 << q)) cnt += t.lcnt[q];
