@@ -58,6 +58,7 @@ rq_status rq_batch_create(rq_ctx_t ctx, const rq_batch_item* items, int n_items,
     for (int i = 0; i < n_items; ++i) {
         const rq_batch_item& it = items[i];
         if (!it.scene || it.count < 0 || (it.count > 0 && (!it.rays || !it.hits))) return RQ_ERR_INVALID_ARG;
+        if (((uintptr_t)it.rays | (uintptr_t)it.hits) & 15u) return RQ_ERR_INVALID_ARG;  // float4 records
         if (it.scene->kind != kind) return RQ_ERR_INVALID_ARG;  // one kernel family per batch
     }
     rq_batch* b = new rq_batch();

@@ -70,8 +70,12 @@ struct TraceParams {
 
 typedef void (*TraceKernelFn)(TraceParams);
 
-TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, bool count);
+// ring: the CWBVH batch kernel that prefetches rays into a per-warp ring in
+// shared memory (for batches of at least kRingMinRaysPerThread rays per
+// thread of the grid; see trace.cu).
+constexpr int64_t kRingMinRaysPerThread = 64;
+TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, bool count, bool ring);
 int smem_entries_of(int requested);
-size_t trace_smem_bytes(rq_bvh_kind kind, int smem_entries, int block);
+size_t trace_smem_bytes(rq_bvh_kind kind, int smem_entries, int block, bool ring);
 
 }  // namespace rq

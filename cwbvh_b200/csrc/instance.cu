@@ -346,6 +346,7 @@ rq_status rq_tlas_buffers(rq_tlas_t tlas, const float** nodes, int64_t* node_flo
 rq_status rq_trace_instanced(rq_ctx_t ctx, rq_tlas_t tlas, const rq_ray* rays, rq_hit* hits, int32_t* instance_out,
                              int64_t count, rq_query query, const rq_launch* launch, void* stream) {
     if (!ctx || !tlas || count < 0 || (count > 0 && (!rays || !hits))) return RQ_ERR_INVALID_ARG;
+    if (((uintptr_t)rays | (uintptr_t)hits) & 15u) return RQ_ERR_INVALID_ARG;  // float4 records
     if (query != RQ_CLOSEST && query != RQ_ANY) return RQ_ERR_INVALID_ARG;
     if (count == 0) return RQ_OK;
     cudaStream_t s = (cudaStream_t)stream;

@@ -89,10 +89,19 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
     if (p.total_rays <= 0) return RQ_OK;
     int dev = 0;
     RQ_CUDA(cudaGetDevice(&dev));
-    TraceKernelFn fn = trace_kernel(kind, q == RQ_ANY, l.smem_stack, multi, count);
-    const size_t smem = trace_smem_bytes(kind, smem_entries_of(l.smem_stack), l.block_size);
-    int nb = blocks_per_sm(fn, l.block_size, smem);
-    if (l.blocks_per_sm > 0) nb = std::min(nb, l.blocks_per_sm);
+    // Batches with many rays per thread take the ring-prefetching kernel.
+    TraceKernelFn fn = nullptr;
+    size_t smem = 0;
+    int nb = 1;
+    auto pick = [&](bool ring) {
+        fn = trace_kernel(kind, q == RQ_ANY, l.smem_stack, multi, count, ring);
+        smem = trace_smem_bytes(kind, smem_entries_of(l.smem_stack), l.block_size, ring);
+        nb = blocks_per_sm(fn, l.block_size, smem);
+        if (l.blocks_per_sm > 0) nb = std::min(nb, l.blocks_per_sm);
+    };
+    const bool ring = kind == RQ_BVH_CWBVH && multi && !count;
+    pick(ring);
+    if (ring && p.total_rays < kRingMinRaysPerThread * device_sms(dev) * nb * l.block_size) pick(false);
     int64_t grid = (int64_t)device_sms(dev) * nb;
     // No more warps than rays need.
     const int64_t warps_needed = (p.total_rays + 31) / 32;
@@ -104,8 +113,10 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
 }
 
 void warm_launch_cache(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool multi, bool count) {
-    TraceKernelFn fn = trace_kernel(kind, q == RQ_ANY, l.smem_stack, multi, count);
-    blocks_per_sm(fn, l.block_size, trace_smem_bytes(kind, smem_entries_of(l.smem_stack), l.block_size));
+    for (int ring = 0; ring <= (kind == RQ_BVH_CWBVH && multi && !count ? 1 : 0); ++ring) {
+        TraceKernelFn fn = trace_kernel(kind, q == RQ_ANY, l.smem_stack, multi, count, ring != 0);
+        blocks_per_sm(fn, l.block_size, trace_smem_bytes(kind, smem_entries_of(l.smem_stack), l.block_size, ring != 0));
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) device_sms(dev);
 }
@@ -339,6 +350,7 @@ static rq_status trace_impl(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, 
                             void* stream, uint32_t* ao_counts = nullptr, int ao_spp = 0) {
     if (!ctx || !scene || count < 0 || (count > 0 && (!rays || (!hits && !ao_counts)))) return RQ_ERR_INVALID_ARG;
     if (query != RQ_CLOSEST && query != RQ_ANY) return RQ_ERR_INVALID_ARG;
+    if (((uintptr_t)rays | (uintptr_t)hits) & 15u) return RQ_ERR_INVALID_ARG;  // float4 records
     if (count == 0) return RQ_OK;
     const rq_launch l = resolve_launch(scene->kind, query, launch);
     TraceParams p = base_params(ctx, l);

@@ -185,6 +185,8 @@ rq_status rq_ctx_check(rq_ctx_t ctx, void* stream);
  * src/TraversalKernelBVH2.cu:190-227): x = t of the closest hit (tmax on a
  * miss), y = Woop address or -1, z/w = u,v of the hit.  RQ_ANY stops a ray at
  * its first accepted triangle; only y != -1 (occluded) is contractual.
+ * Ray and hit buffers are float4 records and must be 16-byte aligned (the
+ * trace and batch calls refuse others with RQ_ERR_INVALID_ARG).
  * Asynchronous on `stream`; errors detected by the kernel surface at rq_ctx_check.
  */
 rq_status rq_trace(rq_ctx_t ctx, rq_scene_t scene, const rq_ray* rays, rq_hit* hits,

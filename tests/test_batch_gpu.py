@@ -137,3 +137,34 @@ def test_autotune_returns_valid_launch(rq, batch_set, tmp_path):
     rq.trace(ctx, ds.scene, rays, b, rq.ANY, launch=l)
     ctx.check()
     assert torch.equal(a[:, 1].view(torch.int32) != -1, b[:, 1].view(torch.int32) != -1)
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+def test_ring_batch_matches_oracle(rq, po, graph):
+    """A batch with at least 64 rays per thread of its grid takes the kernel
+    that prefetches rays into a ring per warp in shared memory (the default
+    large batch).  A grid of one 32-thread block per SM reaches it with a few
+    hundred thousand rays: in the oracle's order its hits equal the oracle's
+    bit for bit, and with the default (full) grid -- the kernel without the
+    ring -- they are the same."""
+    import torch
+    from cwbvh_b200 import workloads as W
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    need = 64 * 32 * sms
+    sizes = [(10, 5000, need // 3 + 17), (11, 60000, need // 3 + 1), (12, 900, 5), (13, 20000, need // 3 + 4001)]
+    bs = []
+    for seed, tris, nrays in sizes:
+        V, I = W.scene_of_size(seed, tris)
+        ds = W.upload(V, I, rq.CWBVH)
+        bs.append((V, I, ds, W.ao_rays(ds, nrays, seed=seed + 1000).contiguous()))
+    assert sum(r.shape[0] for (_, _, _, r) in bs) >= need
+    ctx = rq.Context()
+    narrow = rq.Launch(32, 1, 0, -1.0, 0, 0)  # one 32-thread block per SM, oracle order
+    full = rq.Launch(0, 0, 0, -1.0, 0, 0)
+    for query in (rq.ANY, rq.CLOSEST):
+        got = _run_batch(rq, ctx, bs, query, launch=narrow, sort_threshold=-1, use_graph=graph)
+        ref = _run_batch(rq, ctx, bs, query, launch=full, sort_threshold=-1, use_graph=graph)
+        for (V, I, ds, rays), g, f in zip(bs, got, ref):
+            want = po.trace(0, ds.host.nodes, ds.host.woop, rays.cpu().numpy(), query == rq.ANY)
+            assert np.array_equal(g.view(np.uint32), want.view(np.uint32))
+            assert np.array_equal(f.view(np.uint32), want.view(np.uint32))

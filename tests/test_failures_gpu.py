@@ -124,3 +124,19 @@ def test_bvh2_out_of_range(rq, case):
         ctx.check()
     assert (hits[:, 1].view(np.int32) == -1).all()
     _valid_after(rq, ctx)
+
+
+def test_misaligned_buffers_refused(rq):
+    """Ray and hit buffers are float4 records: a pointer off a 16-byte
+    boundary is refused with RQ_ERR_INVALID_ARG before any launch."""
+    import torch
+    n = cw_node(1, 0, 0, {}, [])
+    scene = rq.Scene.from_arrays(rq.CWBVH, n, np.zeros((3, 4), np.float32))
+    ctx = rq.Context()
+    raw = torch.zeros(64 * 8 + 4, dtype=torch.float32, device="cuda")
+    hits = torch.zeros((64, 4), dtype=torch.float32, device="cuda")
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        rq.trace(ctx, scene, raw[2:2 + 64 * 8].view(64, 8), hits, rq.ANY)
+    with pytest.raises(rq.RQError, match="INVALID_ARG"):
+        rq.trace(ctx, scene, raw[:64 * 8].view(64, 8), raw[2:2 + 64 * 4].view(64, 4), rq.ANY)
+    _valid_after(rq, ctx)
