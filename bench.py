@@ -198,6 +198,27 @@ def measure_l2_read(stream) -> dict:
     return {"peak": best["gbs"], "best": best, "sweep": sweep}
 
 
+def probe_l2_shape(args, warmup: int) -> None:
+    """One shape of the L2 read probe (``--probe-l2 MB,BLOCKS_PER_SM,LOADS``),
+    W + K launches of 16 passes over the buffer each, for an ncu capture of
+    the probe kernel alone; prints its GB/s (CUDA events)."""
+    import torch
+    import cwbvh_b200 as rq
+    mb, bps, loads = (int(x) for x in args.probe_l2.split(","))
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        buf = torch.ones((mb << 20) // 4, dtype=torch.int32, device="cuda")
+        sink = torch.zeros(1, dtype=torch.int32, device="cuda")
+    reps = 16
+
+    def run():
+        rq.check(rq.lib.rq_probe_l2_read_shape(buf.data_ptr(), mb << 20, reps, bps, loads, sink.data_ptr(),
+                                               stream.cuda_stream), "rq_probe_l2_read_shape")
+    ms = time_steps(run, args.steps, warmup, stream)
+    print(json.dumps({"probe": "l2_read", "mbytes": mb, "blocks_per_sm": bps, "loads": loads, "reps": reps,
+                      "ms": round(ms, 4), "gbs": round((mb << 20) * reps / (ms * 1e-3) / 1e9, 1)}), flush=True)
+
+
 def measure_link(mbytes: int = 1024) -> dict:
     """Host link bandwidth with pinned buffers: H2D alone, D2H alone and both
     directions at once on two streams (GB/s), 1 GiB copies."""
@@ -342,6 +363,8 @@ def main():
     ap.add_argument("--ray-cap", type=int, default=0, help="batched: at most this many rays per scene")
     ap.add_argument("--no-configs", action="store_true",
                     help="batched: skip the small, city and large configurations (run in their own processes)")
+    ap.add_argument("--probe-l2", default="",
+                    help="MB,BLOCKS_PER_SM,LOADS: run only the L2 read probe at that shape W+K times (profiler captures)")
     ap.add_argument("--profile", action="store_true",
                     help="batched/small/large: build the workload and only run the trace W+K times (profiler captures)")
     args = ap.parse_args()
@@ -369,6 +392,8 @@ def main():
     import cwbvh_b200 as rq
     from cwbvh_b200 import workloads as W
 
+    if args.probe_l2:
+        return probe_l2_shape(args, warmup)
     if args.workload in ("city", "large", "instanced"):
         {"city": run_city, "large": run_large, "instanced": run_instanced}[args.workload](args, world, rank, dist)
         if dist is not None:
