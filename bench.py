@@ -379,6 +379,18 @@ def main():
     if args.impl == "reference":
         return run_reference(args, world, rank, warmup)
 
+    # ---- the other single-GPU configurations, each in its own process and
+    # before this one opens the device (so no buffer, stream or context of
+    # this process shares the GPU with them): the plain small scene, the city
+    # and the 30M-triangle scene, with their own rooflines
+    configs = None
+    if args.workload == "batched" and not args.quick and world == 1 and not args.no_configs and not args.probe_l2:
+        t0 = time.time()
+        configs = {"config0_plain_small": run_config_process("small", args, warmup),
+                   "config1_city": run_config_process("city", args, warmup),
+                   "config2_large": run_config_process("large", args, warmup)}
+        log(f"[bench] configs 0-2 {time.time()-t0:.1f}s")
+
     import torch
     import torch.distributed as tdist
     import datetime
@@ -598,17 +610,6 @@ def main():
         batching = batching_breakdown(ctx, scenes, rays, hits, ms_batch, stream, warmup)
         batching["small_items"] = batching_small_items(ctx, stream, warmup, args.steps)
         log(f"[bench] batching breakdown {time.time()-t0:.1f}s")
-
-    # ---- the other single-GPU configurations, each in its own process (so
-    # their buffers do not share the device with this one's): the plain small
-    # scene, the city and the 30M-triangle scene, with their own rooflines
-    configs = None
-    if args.workload == "batched" and not args.quick and world == 1 and not args.no_configs:
-        t0 = time.time()
-        configs = {"config0_plain_small": run_config_process("small", args, warmup),
-                   "config1_city": run_config_process("city", args, warmup),
-                   "config2_large": run_config_process("large", args, warmup)}
-        log(f"[bench] configs 0-2 {time.time()-t0:.1f}s")
 
     # ---- CPU baseline (oracle restatement, all host threads, bounded sample)
     cpu = None
