@@ -70,9 +70,9 @@ struct TraceParams {
 
 typedef void (*TraceKernelFn)(TraceParams);
 
-// ring: the CWBVH batch kernel that prefetches rays into a per-warp ring in
-// shared memory (for batches of at least kRingMinRaysPerThread rays per
-// thread of the grid; see trace.cu).
+// ring: the CWBVH any-hit batch kernel that prefetches rays into a per-warp
+// ring in shared memory (for batches of at least kRingMinRaysPerThread rays
+// per thread of the grid; see trace.cu).
 constexpr int64_t kRingMinRaysPerThread = 64;
 TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, bool count, bool ring);
 int smem_entries_of(int requested);

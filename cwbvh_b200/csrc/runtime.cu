@@ -99,7 +99,7 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
         nb = blocks_per_sm(fn, l.block_size, smem);
         if (l.blocks_per_sm > 0) nb = std::min(nb, l.blocks_per_sm);
     };
-    const bool ring = kind == RQ_BVH_CWBVH && multi && !count;
+    const bool ring = kind == RQ_BVH_CWBVH && multi && !count && q == RQ_ANY;
     pick(ring);
     if (ring && p.total_rays < kRingMinRaysPerThread * device_sms(dev) * nb * l.block_size) pick(false);
     int64_t grid = (int64_t)device_sms(dev) * nb;
@@ -113,7 +113,7 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
 }
 
 void warm_launch_cache(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool multi, bool count) {
-    for (int ring = 0; ring <= (kind == RQ_BVH_CWBVH && multi && !count ? 1 : 0); ++ring) {
+    for (int ring = 0; ring <= (kind == RQ_BVH_CWBVH && multi && !count && q == RQ_ANY ? 1 : 0); ++ring) {
         TraceKernelFn fn = trace_kernel(kind, q == RQ_ANY, l.smem_stack, multi, count, ring != 0);
         blocks_per_sm(fn, l.block_size, trace_smem_bytes(kind, smem_entries_of(l.smem_stack), l.block_size, ring != 0));
     }

@@ -52,7 +52,8 @@ constexpr uint32_t kBvh2Sentinel = 0x76543210u;  // src/TraversalKernelBVH2.cu:3
 // ring holds them, which costs a short launch more than the ring saves, so
 // the ring is used from kRingMinRaysPerThread rays per thread of the grid up:
 // +2 % on a batch of 64 scenes with 127M AO rays, +1 % on 64 scenes with
-// 16.8M rays, -6 % on one scene with 1M rays (7 rays per thread).
+// 16.8M rays, -6 % on one scene with 1M rays (7 rays per thread).  Any-hit
+// only: closest-hit batches measured 1 % slower with the ring.
 constexpr unsigned kRingHalf = 32;  // rays per counter add
 constexpr unsigned kRingSlots = 2 * kRingHalf;
 // rays [64][2] float4, the two halves' first global ray index, items [64]
@@ -572,7 +573,11 @@ TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, boo
     if (kind == RQ_BVH_CWBVH) {
         if (count) return select_cwbvh<false, true, false>(any, smem);
         if (!multi) return select_cwbvh<false, false, false>(any, smem);
-        return ring ? select_cwbvh<true, false, true>(any, smem) : select_cwbvh<true, false, false>(any, smem);
+        if (ring && any)  // any-hit batches only (closest-hit measured 1 % slower with the ring)
+            return smem <= 4 ? (TraceKernelFn)cwbvh_kernel<true, 4, true, false, true>
+                             : (smem <= 8 ? (TraceKernelFn)cwbvh_kernel<true, 8, true, false, true>
+                                          : (TraceKernelFn)cwbvh_kernel<true, 16, true, false, true>);
+        return select_cwbvh<true, false, false>(any, smem);
     }
     if (count) return select_bvh2<false, true>(any, smem);
     return multi ? select_bvh2<true, false>(any, smem) : select_bvh2<false, false>(any, smem);

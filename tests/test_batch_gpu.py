@@ -141,12 +141,13 @@ def test_autotune_returns_valid_launch(rq, batch_set, tmp_path):
 
 @pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
 def test_ring_batch_matches_oracle(rq, po, graph):
-    """A batch with at least 64 rays per thread of its grid takes the kernel
-    that prefetches rays into a ring per warp in shared memory (the default
-    large batch).  A grid of one 32-thread block per SM reaches it with a few
-    hundred thousand rays: in the oracle's order its hits equal the oracle's
-    bit for bit, and with the default (full) grid -- the kernel without the
-    ring -- they are the same."""
+    """An any-hit batch with at least 64 rays per thread of its grid takes the
+    kernel that prefetches rays into a ring per warp in shared memory (the
+    default large AO batch).  A grid of one 32-thread block per SM reaches it
+    with a few hundred thousand rays: in the oracle's order its hits equal the
+    oracle's bit for bit, and with the default (full) grid -- the kernel
+    without the ring -- they are the same.  Closest-hit batches of the same
+    shape (always without the ring) are checked alike."""
     import torch
     from cwbvh_b200 import workloads as W
     sms = torch.cuda.get_device_properties(0).multi_processor_count
