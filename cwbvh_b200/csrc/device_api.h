@@ -70,10 +70,12 @@ struct TraceParams {
 
 typedef void (*TraceKernelFn)(TraceParams);
 
-// ring: the CWBVH any-hit batch kernel that prefetches rays into a per-warp
-// ring in shared memory (for batches of at least kRingMinRaysPerThread rays
-// per thread of the grid; see trace.cu).
+// ring: the CWBVH any-hit kernel that prefetches rays into a per-warp ring
+// in shared memory (see trace.cu), for batches of at least
+// kRingMinRaysPerThread rays per thread of the grid and single-scene launches
+// of at least kRingMinRaysPerThreadSingle (which have no item search to hide).
 constexpr int64_t kRingMinRaysPerThread = 64;
+constexpr int64_t kRingMinRaysPerThreadSingle = 256;
 TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, bool count, bool ring);
 int smem_entries_of(int requested);
 size_t trace_smem_bytes(rq_bvh_kind kind, int smem_entries, int block, bool ring);

@@ -89,7 +89,7 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
     if (p.total_rays <= 0) return RQ_OK;
     int dev = 0;
     RQ_CUDA(cudaGetDevice(&dev));
-    // Batches with many rays per thread take the ring-prefetching kernel.
+    // Any-hit launches with many rays per thread take the ring-prefetching kernel.
     TraceKernelFn fn = nullptr;
     size_t smem = 0;
     int nb = 1;
@@ -99,9 +99,11 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
         nb = blocks_per_sm(fn, l.block_size, smem);
         if (l.blocks_per_sm > 0) nb = std::min(nb, l.blocks_per_sm);
     };
-    const bool ring = kind == RQ_BVH_CWBVH && multi && !count && q == RQ_ANY;
+    const bool ring = kind == RQ_BVH_CWBVH && !count && q == RQ_ANY;
     pick(ring);
-    if (ring && p.total_rays < kRingMinRaysPerThread * device_sms(dev) * nb * l.block_size) pick(false);
+    if (ring && p.total_rays < (multi ? kRingMinRaysPerThread : kRingMinRaysPerThreadSingle) * device_sms(dev) * nb *
+                                   l.block_size)
+        pick(false);
     int64_t grid = (int64_t)device_sms(dev) * nb;
     // No more warps than rays need.
     const int64_t warps_needed = (p.total_rays + 31) / 32;
@@ -113,7 +115,7 @@ rq_status launch_trace(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool mu
 }
 
 void warm_launch_cache(rq_bvh_kind kind, rq_query q, const rq_launch& l, bool multi, bool count) {
-    for (int ring = 0; ring <= (kind == RQ_BVH_CWBVH && multi && !count && q == RQ_ANY ? 1 : 0); ++ring) {
+    for (int ring = 0; ring <= (kind == RQ_BVH_CWBVH && !count && q == RQ_ANY ? 1 : 0); ++ring) {
         TraceKernelFn fn = trace_kernel(kind, q == RQ_ANY, l.smem_stack, multi, count, ring != 0);
         blocks_per_sm(fn, l.block_size, trace_smem_bytes(kind, smem_entries_of(l.smem_stack), l.block_size, ring != 0));
     }

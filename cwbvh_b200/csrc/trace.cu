@@ -41,7 +41,7 @@ constexpr uint32_t kBvh2Sentinel = 0x76543210u;  // src/TraversalKernelBVH2.cu:3
 
 // ------------------------------------------------- per-warp ray prefetch --
 //
-// The CWBVH batch kernels of large batches (RING) take rays 32 at a time per
+// The CWBVH any-hit kernels of large launches (RING) take rays 32 at a time per
 // warp (one counter add per 32 rays) into a ring of 64 slots per warp in
 // shared memory: two halves, each filled by one cp.async group (every lane
 // copies one ray's 32 bytes and notes its batch item).  A refill hands idle
@@ -50,10 +50,13 @@ constexpr uint32_t kBvh2Sentinel = 0x76543210u;  // src/TraversalKernelBVH2.cu:3
 // the item search sits on its path.  A half is refilled as soon as its last
 // slot is handed out.  The last rays of a launch stay tied to the warp whose
 // ring holds them, which costs a short launch more than the ring saves, so
-// the ring is used from kRingMinRaysPerThread rays per thread of the grid up:
-// +2 % on a batch of 64 scenes with 127M AO rays, +1 % on 64 scenes with
-// 16.8M rays, -6 % on one scene with 1M rays (7 rays per thread).  Any-hit
-// only: closest-hit batches measured 1 % slower with the ring.
+// the ring is used from kRingMinRaysPerThread rays per thread of the grid up
+// (batches) and from kRingMinRaysPerThreadSingle up (one scene, where no item
+// search is saved): +2 % on a batch of 64 scenes with 127M AO rays, +1 % on
+// 64 scenes with 16.8M rays, +1.6 % on one 29.6M-triangle scene with 64M AO
+// rays (440 per thread), -0.5 % on one scene with 16.8M rays (110 per
+// thread), -6 % on one scene with 1M rays (7 per thread).  Any-hit only:
+// closest-hit batches measured 1 % slower with the ring.
 constexpr unsigned kRingHalf = 32;  // rays per counter add
 constexpr unsigned kRingSlots = 2 * kRingHalf;
 // rays [64][2] float4, the two halves' first global ray index, items [64]
@@ -572,11 +575,16 @@ static TraceKernelFn select_bvh2(bool any, int smem) {
 TraceKernelFn trace_kernel(rq_bvh_kind kind, bool any, int smem, bool multi, bool count, bool ring) {
     if (kind == RQ_BVH_CWBVH) {
         if (count) return select_cwbvh<false, true, false>(any, smem);
+        if (ring && any) {  // any-hit only (closest-hit batches measured 1 % slower with the ring)
+            if (multi)
+                return smem <= 4 ? (TraceKernelFn)cwbvh_kernel<true, 4, true, false, true>
+                                 : (smem <= 8 ? (TraceKernelFn)cwbvh_kernel<true, 8, true, false, true>
+                                              : (TraceKernelFn)cwbvh_kernel<true, 16, true, false, true>);
+            return smem <= 4 ? (TraceKernelFn)cwbvh_kernel<true, 4, false, false, true>
+                             : (smem <= 8 ? (TraceKernelFn)cwbvh_kernel<true, 8, false, false, true>
+                                          : (TraceKernelFn)cwbvh_kernel<true, 16, false, false, true>);
+        }
         if (!multi) return select_cwbvh<false, false, false>(any, smem);
-        if (ring && any)  // any-hit batches only (closest-hit measured 1 % slower with the ring)
-            return smem <= 4 ? (TraceKernelFn)cwbvh_kernel<true, 4, true, false, true>
-                             : (smem <= 8 ? (TraceKernelFn)cwbvh_kernel<true, 8, true, false, true>
-                                          : (TraceKernelFn)cwbvh_kernel<true, 16, true, false, true>);
         return select_cwbvh<true, false, false>(any, smem);
     }
     if (count) return select_bvh2<false, true>(any, smem);

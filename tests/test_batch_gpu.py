@@ -169,3 +169,25 @@ def test_ring_batch_matches_oracle(rq, po, graph):
             want = po.trace(0, ds.host.nodes, ds.host.woop, rays.cpu().numpy(), query == rq.ANY)
             assert np.array_equal(g.view(np.uint32), want.view(np.uint32))
             assert np.array_equal(f.view(np.uint32), want.view(np.uint32))
+
+
+def test_ring_single_scene_matches_oracle(rq, po):
+    """A single-scene any-hit launch with at least 256 rays per thread of its
+    grid takes the ring-prefetching kernel too: bit for bit the oracle's hits
+    in its order, and the same as the kernel without the ring (full grid)."""
+    import torch
+    from cwbvh_b200 import workloads as W
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n = 256 * 32 * sms + 777
+    V, I = W.scene_of_size(21, 30000)
+    ds = W.upload(V, I, rq.CWBVH)
+    rays = W.ao_rays(ds, n, seed=1021).contiguous()
+    ctx = rq.Context()
+    got = torch.full((n, 4), float("nan"), device="cuda")
+    ref = torch.full((n, 4), float("nan"), device="cuda")
+    rq.trace(ctx, ds.scene, rays, got, rq.ANY, launch=rq.Launch(32, 1, 0, -1.0, 0, 0))
+    rq.trace(ctx, ds.scene, rays, ref, rq.ANY, launch=rq.Launch(0, 0, 0, -1.0, 0, 0))
+    ctx.check()
+    want = po.trace(0, ds.host.nodes, ds.host.woop, rays.cpu().numpy(), True)
+    assert np.array_equal(got.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    assert torch.equal(got.view(torch.int32), ref.view(torch.int32))
