@@ -384,7 +384,8 @@ def main():
     # this process shares the GPU with them): the plain small scene, the city
     # and the 30M-triangle scene, with their own rooflines
     configs = None
-    if args.workload == "batched" and not args.quick and world == 1 and not args.no_configs and not args.probe_l2:
+    if (args.workload == "batched" and not args.quick and world == 1 and not args.no_configs and not args.probe_l2
+            and not args.profile and args.subset == 0 and args.ray_cap == 0):
         t0 = time.time()
         configs = {"config0_plain_small": run_config_process("small", args, warmup),
                    "config1_city": run_config_process("city", args, warmup),
