@@ -471,6 +471,7 @@ def main():
     t0 = time.time()
     bp = rq.autotune_batch(ctx, items, rq.ANY, cache_path=cache, stream=stream)
     log(f"[bench] autotune {time.time()-t0:.1f}s -> block {bp.launch.block_size} smem {bp.launch.smem_stack} "
+        f"postpone {bp.launch.postpone_ratio:.2f} fetch {bp.launch.fetch_nd}/{bp.launch.fetch_nw} "
         f"sort_threshold {bp.sort_threshold} graph {bp.use_graph}")
     batch = rq.Batch(ctx, items, rq.ANY, params=bp)
     ms_batch = time_steps(lambda: batch.run(stream), args.steps, warmup, stream, dist, flush)
@@ -563,8 +564,11 @@ def main():
             # This library's closest-hit batch on the same rays: the like-for-like figure, and the
             # closest triangles compared with the reference kernel's.
             chits = [torch.empty_like(h) for h in hits]
-            cbatch = rq.Batch(ctx, [(ds.scene, r, h) for ds, r, h in zip(scenes, rays, chits)], rq.CLOSEST,
-                              params=bp)
+            citems = [(ds.scene, r, h) for ds, r, h in zip(scenes, rays, chits)]
+            # closest-hit gets its own autotuned launch (refill and postponing
+            # settings that suit any-hit need not suit closest-hit)
+            cbp = rq.autotune_batch(ctx, citems, rq.CLOSEST, cache_path=cache, stream=stream)
+            cbatch = rq.Batch(ctx, citems, rq.CLOSEST, params=cbp)
             ms_closest = time_steps(lambda: cbatch.run(stream), args.steps, warmup, stream, dist, flush)
             ctx.check(stream)
             same = total_n = bad_mine = bad_ref = 0
@@ -581,7 +585,11 @@ def main():
                 total_n += int(a.numel())
             ref_gpu["this_library_closest_hit"] = {
                 "value": round(total_rays / (ms_closest * 1e-3) / 1e6, 2), "unit": "Mrays/s",
-                "ms_per_step": round(ms_closest, 4), "launch": "one persistent batch, the any-hit autotuned shape",
+                "ms_per_step": round(ms_closest, 4),
+                "launch": {"block": cbp.launch.block_size, "smem_stack": cbp.launch.smem_stack,
+                           "postpone_ratio": round(cbp.launch.postpone_ratio, 3),
+                           "fetch_nd_nw": [cbp.launch.fetch_nd, cbp.launch.fetch_nw],
+                           "what": "one persistent batch, autotuned for closest-hit"},
                 "closest_prim_ids_equal_frac": round(same / max(total_n, 1), 6),
                 "hit_addresses_outside_the_primitive_map": {"this_library": bad_mine, "reference": bad_ref}}
             ref_gpu["closest_vs_reference_kernel"] = round(total_rays / (ms_closest * 1e-3) / 1e6 / ref_gpu["value"],
@@ -644,6 +652,8 @@ def main():
             "query": "any-hit",
             "layout": "CWBVH 80 B nodes, Woop 48 B triangles, Ray 32 B, Hit 16 B",
             "launch": {"block": bp.launch.block_size, "smem_stack": bp.launch.smem_stack,
+                       "postpone_ratio": round(bp.launch.postpone_ratio, 3),
+                       "fetch_nd_nw": [bp.launch.fetch_nd, bp.launch.fetch_nw],
                        "sort_threshold": int(bp.sort_threshold), "cuda_graph": bool(bp.use_graph)},
             "l2": ("inputs larger than L2 (rays+hits %.1f GB per step)" % (total_rays * 48 / 1e9)) if flush is None
             else "L2 flushed before every timed step (256 MB write outside the events; rays+hits are 48 MB)",

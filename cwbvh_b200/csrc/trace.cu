@@ -155,7 +155,7 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
     const unsigned tid = threadIdx.x;
     const unsigned B = blockDim.x;
 
-    constexpr bool PAIRS = !(MULTI && RING);
+    constexpr bool PAIRS = !MULTI;
     Lane L{};
     float ox = 0.f, oy = 0.f, oz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f, tmin = 0.f, tmax = 0.f;
     float idx_ = 0.f, idy = 0.f, idz = 0.f;
@@ -356,10 +356,10 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
                         // has two (PAIRS), in the group's order: the second is
                         // tested against the tmax the first left, and not at
                         // all once an any-hit ray has finished (fewer
-                        // warp-wide votes per triangle: +1.0-1.6 % on single
-                        // scenes and small-item batches; the 64-scene AO
-                        // batch measured 0.5-1.1 % slower, so its ring batch
-                        // kernel tests one per round).
+                        // warp-wide votes per triangle: +1.0-2.2 % on single
+                        // scenes; batches measured slower with it -- the
+                        // 64-scene AO batch 0.5-1.1 %, its closest-hit twin
+                        // 10 % -- so batch kernels test one per round).
                         const unsigned ti = highest_bit(tg.y);
                         const unsigned tri = tg.x * 3u + ti * 3u;
                         tg.y &= ~(1u << ti);
