@@ -9,8 +9,8 @@
 // src/TraversalKernelCWBVH.cu:56-87, written with __shfl_sync instead of a
 // volatile shared word so it is correct under independent thread scheduling).
 // A warp re-fills after the idle lanes have cost Nw lane-iterations beyond Nd
-// (src/TraversalKernelCWBVH.cu:365-371).  Large CWBVH batches take their rays
-// through a per-warp ring of prefetched rays instead (below).  Every vote is
+// (src/TraversalKernelCWBVH.cu:365-371).  Large CWBVH any-hit launches take
+// their rays through a per-warp ring of prefetched rays instead (below).  Every vote is
 // over the full warp and every loop is warp-uniform, so lanes never diverge
 // around a collective.
 //
