@@ -155,7 +155,7 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
     const unsigned tid = threadIdx.x;
     const unsigned B = blockDim.x;
 
-    constexpr bool PAIRS = !MULTI;
+    constexpr bool PAIRS = !(MULTI && RING);
     Lane L{};
     float ox = 0.f, oy = 0.f, oz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f, tmin = 0.f, tmax = 0.f;
     float idx_ = 0.f, idy = 0.f, idz = 0.f;
@@ -357,9 +357,10 @@ __global__ void RQ_KERNEL_BOUNDS cwbvh_kernel(const TraceParams p) {
                         // tested against the tmax the first left, and not at
                         // all once an any-hit ray has finished (fewer
                         // warp-wide votes per triangle: +1.0-2.2 % on single
-                        // scenes; batches measured slower with it -- the
-                        // 64-scene AO batch 0.5-1.1 %, its closest-hit twin
-                        // 10 % -- so batch kernels test one per round).
+                        // scenes, +1.3 % on the 64-scene closest-hit batch,
+                        // +2.0 % on a one-item batch; the ring batch kernel
+                        // measured 0.5-1.1 % slower with it on the 64-scene
+                        // AO batch and tests one per round).
                         const unsigned ti = highest_bit(tg.y);
                         const unsigned tri = tg.x * 3u + ti * 3u;
                         tg.y &= ~(1u << ti);
